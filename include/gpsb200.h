@@ -1,0 +1,237 @@
+/* gpsb200: B200-native stochastic particle renderer for 3D Gaussian splats (GPS / PBVR).
+ *
+ * C ABI of the drop-in replacement for the wgpu renderer of gps-pbvr-web
+ * (crates/gps-render/src/gps.rs, sorted.rs). Every entry point takes plain pointers and
+ * sizes, returns a gpsb_status, and never aborts on user input; the message of the last
+ * failure is available from gpsb_last_error(). One renderer is owned by one host thread and
+ * runs its GPU work on its own CUDA stream (or a stream the caller supplies).
+ *
+ * Citations are file:line in the reference project.
+ */
+#ifndef GPSB200_H
+#define GPSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------ status */
+typedef enum gpsb_status {
+    GPSB_OK = 0,
+    GPSB_ERR_INVALID_ARGUMENT = 1, /* bad size, null pointer, mismatched spp_side ... */
+    GPSB_ERR_LIMIT = 2,            /* scene / resolution above a limit (gps.rs:572-590, 696-701) */
+    GPSB_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+    GPSB_ERR_OUT_OF_MEMORY = 4,
+    GPSB_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up (error word set) */
+    GPSB_ERR_STATE = 6,            /* call not valid in the current state (e.g. no sorted render yet) */
+    GPSB_ERR_PARSE = 7             /* PLY parse error (crates/gps-io/src/lib.rs:17-27) */
+} gpsb_status;
+
+/* ------------------------------------------------------------------------------ types */
+/* One splat, 64 bytes, identical to GpuGaussian (gps.rs:26-38). */
+typedef struct gpsb_gaussian {
+    float pos_opacity[4]; /* xyz position, w = activated opacity */
+    float log_scale[4];   /* xyz log of the per-axis standard deviation */
+    float rot_wxyz[4];    /* (w, x, y, z), normalised by the renderer */
+    float color[4];       /* xyz linear SH0 colour = f_dc * SH_C0 + 0.5 */
+} gpsb_gaussian;
+
+/* Pinhole camera of the oracle (crates/gps-core/src/oracle.rs:33-48): cam = view_rot *
+ * (world - view_pos), +Z forward, image +Y down. A principal point of exactly (0, 0) means
+ * the image centre (gps.rs:818). view_rot is row-major. */
+typedef struct gpsb_camera {
+    double view_rot[9];
+    double view_pos[3];
+    double focal_x, focal_y;
+    double cx, cy;
+    double low_pass; /* px^2 added to the projected covariance diagonal (default 0.3) */
+} gpsb_camera;
+
+/* Method indices (gps.rs:104-127). */
+enum {
+    GPSB_METHOD_GPS = 0,
+    GPSB_METHOD_PROPORTIONAL = 1,
+    GPSB_METHOD_EXTINCTION = 2,
+    GPSB_METHOD_VIEW_CONDITIONED = 3,
+    GPSB_METHOD_SCREEN_OCCUPANCY = 4
+};
+/* Calibration levels C0..C3 (gps.rs:144-165). */
+enum {
+    GPSB_CAL_NONE = 0,
+    GPSB_CAL_OBJECT_ZOOM = 1,
+    GPSB_CAL_PER_SPLAT_DEPTH = 2,
+    GPSB_CAL_PER_SPLAT_FOOTPRINT = 3
+};
+/* RenderPath (gps.rs:93-100): the splat-parallel primitive path is the validation path. */
+enum { GPSB_PATH_PRIMITIVE = 0, GPSB_PATH_PARTICLE = 1 };
+
+/* PbvrParams (gps.rs:169-185). Booleans are 0/1. */
+typedef struct gpsb_pbvr_params {
+    uint32_t calibration;
+    uint32_t radial_correction;
+    uint32_t centre_depth;
+    uint32_t low_pass_jitter;
+    float base_k;
+    float reference_pixel_length;
+} gpsb_pbvr_params;
+
+/* RenderParams (gps.rs:189-229). */
+typedef struct gpsb_params {
+    uint32_t spp_side;             /* subpixels per pixel = spp_side^2, 1..4 */
+    float density_scale;
+    uint32_t max_points_per_splat;
+    float near_z;
+    float background[3];
+    float exposure;
+    uint32_t srgb_output;
+    uint32_t exact_radius;
+    uint32_t sh_degree;
+    uint32_t path;
+    uint32_t method;
+    gpsb_pbvr_params pbvr;
+} gpsb_params;
+
+/* GpuStats (gps.rs:231-272): cumulative since gpsb_reset_stats. */
+typedef struct gpsb_stats {
+    uint64_t points;
+    uint64_t truncated_splats;
+    uint64_t dropped_points;
+    uint64_t visible_splats;
+    uint64_t orphan_subpixels;
+    uint64_t candidates;
+    uint64_t undercovered_splats;
+    uint64_t skipped_ensembles;
+    uint64_t ensembles;
+    uint64_t probe_demand;
+    uint32_t issue;
+    uint32_t _pad;
+} gpsb_stats;
+
+typedef struct gpsb_renderer gpsb_renderer;
+
+/* --------------------------------------------------------------------- defaults / misc */
+/* RenderParams::default() and PbvrParams::default() (gps.rs:181-228). */
+void gpsb_params_default(gpsb_params* out);
+/* Library version string. */
+const char* gpsb_version(void);
+/* Message of the last failure of `r` (or of the last gpsb_create / free function when r is NULL). */
+const char* gpsb_last_error(const gpsb_renderer* r);
+
+/* OracleCamera::look_at (crates/gps-core/src/oracle.rs:53-70). fov_y in radians. */
+gpsb_status gpsb_camera_look_at(const double eye[3], const double target[3], const double up[3],
+                                double fov_y, uint32_t w, uint32_t h, gpsb_camera* out);
+/* OrbitCamera::to_camera (crates/gps-core/src/camera.rs:31-65). */
+gpsb_status gpsb_orbit_camera(const double target[3], double distance, double yaw, double pitch,
+                              const double up[3], double fov_y, uint32_t w, uint32_t h,
+                              gpsb_camera* out);
+/* OrbitCamera::robust_sphere (camera.rs:70-84) over xyz of n splats. */
+gpsb_status gpsb_robust_sphere(const gpsb_gaussian* splats, size_t n, double centre[3], double* radius);
+
+/* gps_core::radius_lut (crates/gps-core/src/lib.rs:624-636): 65 x 129 f32 table. */
+gpsb_status gpsb_radius_lut(float* out_8385);
+
+/* Estimated per-frame GPU bytes (gps.rs:288-291): depth+winner, accum, splats. */
+void gpsb_estimate_memory(uint32_t w, uint32_t h, uint32_t spp_side, size_t n_splats,
+                          uint64_t* depth_winner_bytes, uint64_t* accum_bytes, uint64_t* splat_bytes);
+
+/* ------------------------------------------------------------------- construction */
+/* GpsRenderer::new (gps.rs:380-570). spp_side is clamped to 1..4. device = CUDA ordinal. */
+gpsb_status gpsb_create(int device, uint32_t width, uint32_t height, uint32_t spp_side,
+                        gpsb_renderer** out);
+/* Releases every GPU resource of `r` (Drop of GpsRenderer). NULL is a no-op. */
+void gpsb_destroy(gpsb_renderer* r);
+/* Run the renderer's work on an external cudaStream_t (NULL restores its own stream). */
+gpsb_status gpsb_set_stream(gpsb_renderer* r, void* cuda_stream);
+
+/* ------------------------------------------------------------------- scene */
+/* GpsRenderer::set_gaussians (gps.rs:683). Host pointer. On error the old scene stays. */
+gpsb_status gpsb_set_gaussians(gpsb_renderer* r, const gpsb_gaussian* splats, size_t n);
+/* GpsRenderer::set_gaussians_sh (gps.rs:689-740): sh_rest holds 3*((d+1)^2-1) floats per
+ * splat, channel-major (R.., G.., B..); sh_len must equal n*3*((d+1)^2-1) when degree >= 1. */
+gpsb_status gpsb_set_gaussians_sh(gpsb_renderer* r, const gpsb_gaussian* splats, size_t n,
+                                  const float* sh_rest, size_t sh_len, uint32_t degree);
+/* The same from device pointers (no host staging). */
+gpsb_status gpsb_set_gaussians_sh_device(gpsb_renderer* r, const void* splats_dev, size_t n,
+                                         const void* sh_rest_dev, size_t sh_len, uint32_t degree);
+
+/* GpsRenderer::resize (gps.rs:781-789): reallocates per-frame buffers, resets history. */
+gpsb_status gpsb_resize(gpsb_renderer* r, uint32_t width, uint32_t height, uint32_t spp_side);
+/* reset_accum (gps.rs:792-801) also restarts the skipped-ensemble counter. */
+gpsb_status gpsb_reset_accum(gpsb_renderer* r);
+/* reset_stats (gps.rs:803-809). */
+gpsb_status gpsb_reset_stats(gpsb_renderer* r);
+
+/* ------------------------------------------------------------------- render */
+/* GpsRenderer::render_ensembles (gps.rs:861-925): `count` independent ensembles with seeds
+ * first_seed .. first_seed+count-1 accumulated into the history. The reference accepts at
+ * most 4 per call (gps.rs:19); any count is accepted here and batched on the device. */
+gpsb_status gpsb_render_ensembles(gpsb_renderer* r, const gpsb_camera* cam, const gpsb_params* p,
+                                  uint32_t first_seed, uint32_t count);
+/* Batched trajectory (no reference counterpart; the frame loop of gps-web renders one camera
+ * at a time): for every camera c, ensembles first_seed .. first_seed+E-1 are accumulated into
+ * a fresh accumulation written to accum_out_dev + c*W*H*4 floats (device pointer, RGB sum and
+ * count like read_accum). The renderer's own history is not touched. */
+gpsb_status gpsb_render_trajectory(gpsb_renderer* r, const gpsb_camera* cams, uint32_t n_cams,
+                                   const gpsb_params* p, uint32_t first_seed,
+                                   uint32_t ensembles_per_camera, void* accum_out_dev);
+/* render_sorted (gps.rs:930-944): depth-sorted alpha image written into the history with
+ * count 1 and reported as `as_ensembles` accumulated ensembles. */
+gpsb_status gpsb_render_sorted(gpsb_renderer* r, const gpsb_camera* cam, const gpsb_params* p,
+                               uint32_t as_ensembles);
+/* probe_demand (gps.rs:948-955): GPS particle demand of the view into stats.probe_demand. */
+gpsb_status gpsb_probe_demand(gpsb_renderer* r, const gpsb_camera* cam, const gpsb_params* p);
+
+/* ------------------------------------------------------------------- readback */
+/* read_accum (gps.rs:989-993): W*H*4 floats (RGB sum, A = count). Host pointer. Synchronises. */
+gpsb_status gpsb_read_accum(gpsb_renderer* r, float* rgba_host);
+/* Device pointer of the accumulation buffer (valid until the next resize/destroy). */
+gpsb_status gpsb_accum_device_ptr(gpsb_renderer* r, void** out);
+/* read_stats (gps.rs:996-1000). Synchronises. */
+gpsb_status gpsb_read_stats(gpsb_renderer* r, gpsb_stats* out);
+/* request_stats / latest_stats / stats_issued (gps.rs:1005-1038): one readback in flight. */
+gpsb_status gpsb_request_stats(gpsb_renderer* r);
+gpsb_status gpsb_latest_stats(gpsb_renderer* r, gpsb_stats* out);
+uint32_t gpsb_stats_issued(const gpsb_renderer* r);
+/* read_sorted test hook (gps.rs:958-963): n keys and n values of the last sorted render. */
+gpsb_status gpsb_read_sorted(gpsb_renderer* r, uint32_t* keys, uint32_t* vals);
+/* accumulated() = submitted - skipped (gps.rs:675-677); submitted() (gps.rs:669-671). */
+uint32_t gpsb_accumulated(gpsb_renderer* r);
+uint32_t gpsb_submitted(const gpsb_renderer* r);
+/* wait_idle (gps.rs:1055-1057). */
+gpsb_status gpsb_sync(gpsb_renderer* r);
+/* composite (gps.rs:967-986, shaders/gps_composite.wgsl) into a headless RGBA8 buffer of
+ * out_w x out_h (bilinear up/down-sampling in linear space, exposure, optional sRGB OETF). */
+gpsb_status gpsb_composite_rgba8(gpsb_renderer* r, const gpsb_params* p, uint32_t out_w,
+                                 uint32_t out_h, uint8_t* out_host);
+
+/* ------------------------------------------------------------------- queries */
+void gpsb_size(const gpsb_renderer* r, uint32_t* w, uint32_t* h, uint32_t* spp_side);
+uint32_t gpsb_gaussian_count(const gpsb_renderer* r);
+uint32_t gpsb_sh_max_degree(const gpsb_renderer* r);
+uint64_t gpsb_sh_bytes(const gpsb_renderer* r);
+
+/* ------------------------------------------------------------------- test hooks */
+/* Per-splat particle counts (after the cap) of ensemble `slot` of the last particle-path
+ * render call (slot < min(count, batch)); n entries. Used by the bit-exact parity tests. */
+gpsb_status gpsb_debug_read_counts(gpsb_renderer* r, uint32_t slot, uint32_t* counts);
+/* Packed subpixel winners ((depth key << 32) | splat id, all ones = empty) of ensemble
+ * `slot` of the last render call; W*H*spp entries. */
+gpsb_status gpsb_debug_read_subpixels(gpsb_renderer* r, uint32_t slot, uint64_t* packed);
+/* Device-side error word (bounded waits that gave up); 0 when healthy. */
+uint32_t gpsb_debug_error_word(gpsb_renderer* r);
+
+/* ------------------------------------------------------------------- PLY (gps-io) */
+/* load_ply (crates/gps-io/src/lib.rs:260-338) + activation (lib.rs:84-96) +
+ * GpuGaussian::from_activated (gps.rs:41-49), parsed on the host. Two calls: first with
+ * outputs NULL to get n and the SH degree, then with buffers of n splats and
+ * n*3*((d+1)^2-1) SH floats. */
+gpsb_status gpsb_load_ply(const uint8_t* bytes, size_t len, size_t* n_out, uint32_t* sh_degree_out,
+                          gpsb_gaussian* splats, float* sh_rest);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPSB200_H */
