@@ -1,0 +1,121 @@
+"""ctypes declarations of include/gpsb200.h and the loader of libgpsb200.so.
+
+The library is built in-tree (gps-pbvr-web_b200/build.py). Loading fails loudly when it is
+missing: there is no CPU fallback of the renderer.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpsb200.so")
+
+GPSB_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "LIMIT", 3: "CUDA", 4: "OUT_OF_MEMORY", 5: "TIMEOUT",
+                6: "STATE", 7: "PARSE"}
+
+
+class Gaussian(C.Structure):
+    _fields_ = [("pos_opacity", C.c_float * 4), ("log_scale", C.c_float * 4), ("rot_wxyz", C.c_float * 4),
+                ("color", C.c_float * 4)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("view_rot", C.c_double * 9), ("view_pos", C.c_double * 3), ("focal_x", C.c_double),
+                ("focal_y", C.c_double), ("cx", C.c_double), ("cy", C.c_double), ("low_pass", C.c_double)]
+
+
+class PbvrParamsC(C.Structure):
+    _fields_ = [("calibration", C.c_uint32), ("radial_correction", C.c_uint32), ("centre_depth", C.c_uint32),
+                ("low_pass_jitter", C.c_uint32), ("base_k", C.c_float), ("reference_pixel_length", C.c_float)]
+
+
+class ParamsC(C.Structure):
+    _fields_ = [("spp_side", C.c_uint32), ("density_scale", C.c_float), ("max_points_per_splat", C.c_uint32),
+                ("near_z", C.c_float), ("background", C.c_float * 3), ("exposure", C.c_float),
+                ("srgb_output", C.c_uint32), ("exact_radius", C.c_uint32), ("sh_degree", C.c_uint32),
+                ("path", C.c_uint32), ("method", C.c_uint32), ("pbvr", PbvrParamsC)]
+
+
+class StatsC(C.Structure):
+    _fields_ = [("points", C.c_uint64), ("truncated_splats", C.c_uint64), ("dropped_points", C.c_uint64),
+                ("visible_splats", C.c_uint64), ("orphan_subpixels", C.c_uint64), ("candidates", C.c_uint64),
+                ("undercovered_splats", C.c_uint64), ("skipped_ensembles", C.c_uint64), ("ensembles", C.c_uint64),
+                ("probe_demand", C.c_uint64), ("issue", C.c_uint32), ("_pad", C.c_uint32)]
+
+
+P = C.c_void_p
+U32 = C.c_uint32
+SZ = C.c_size_t
+ST = C.c_int
+
+# name -> (restype, argtypes); every function declared in include/gpsb200.h
+SIGNATURES = {
+    "gpsb_params_default": (None, [P]),
+    "gpsb_version": (C.c_char_p, []),
+    "gpsb_last_error": (C.c_char_p, [P]),
+    "gpsb_camera_look_at": (ST, [P, P, P, C.c_double, U32, U32, P]),
+    "gpsb_orbit_camera": (ST, [P, C.c_double, C.c_double, C.c_double, P, C.c_double, U32, U32, P]),
+    "gpsb_robust_sphere": (ST, [P, SZ, P, P]),
+    "gpsb_radius_lut": (ST, [P]),
+    "gpsb_estimate_memory": (None, [U32, U32, U32, SZ, P, P, P]),
+    "gpsb_create": (ST, [C.c_int, U32, U32, U32, P]),
+    "gpsb_destroy": (None, [P]),
+    "gpsb_set_stream": (ST, [P, P]),
+    "gpsb_set_gaussians": (ST, [P, P, SZ]),
+    "gpsb_set_gaussians_sh": (ST, [P, P, SZ, P, SZ, U32]),
+    "gpsb_set_gaussians_sh_device": (ST, [P, P, SZ, P, SZ, U32]),
+    "gpsb_resize": (ST, [P, U32, U32, U32]),
+    "gpsb_reset_accum": (ST, [P]),
+    "gpsb_reset_stats": (ST, [P]),
+    "gpsb_render_ensembles": (ST, [P, P, P, U32, U32]),
+    "gpsb_render_trajectory": (ST, [P, P, U32, P, U32, U32, P]),
+    "gpsb_render_sorted": (ST, [P, P, P, U32]),
+    "gpsb_probe_demand": (ST, [P, P, P]),
+    "gpsb_read_accum": (ST, [P, P]),
+    "gpsb_accum_device_ptr": (ST, [P, P]),
+    "gpsb_read_stats": (ST, [P, P]),
+    "gpsb_request_stats": (ST, [P]),
+    "gpsb_latest_stats": (ST, [P, P]),
+    "gpsb_stats_issued": (U32, [P]),
+    "gpsb_read_sorted": (ST, [P, P, P]),
+    "gpsb_accumulated": (U32, [P]),
+    "gpsb_submitted": (U32, [P]),
+    "gpsb_sync": (ST, [P]),
+    "gpsb_composite_rgba8": (ST, [P, P, U32, U32, P]),
+    "gpsb_size": (None, [P, P, P, P]),
+    "gpsb_gaussian_count": (U32, [P]),
+    "gpsb_sh_max_degree": (U32, [P]),
+    "gpsb_sh_bytes": (C.c_uint64, [P]),
+    "gpsb_debug_read_counts": (ST, [P, U32, P]),
+    "gpsb_debug_read_subpixels": (ST, [P, U32, P]),
+    "gpsb_debug_error_word": (U32, [P]),
+    "gpsb_load_ply": (ST, [P, SZ, P, P, P, P]),
+    "gpsb_ply_last_error": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded renderer library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python gps-pbvr-web_b200/build.py` "
+                               "(the renderer has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def header_functions(header_path=None):
+    """Function names declared in include/gpsb200.h (for the export check)."""
+    import re
+    path = header_path or os.path.join(os.path.dirname(HERE), "include", "gpsb200.h")
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(gpsb_[a-z0-9_]+)\s*\(", text)))

@@ -1,0 +1,705 @@
+// Particle-path kernels for sm_100a: geometry (once per camera), Poisson counts fused with a
+// single-pass decoupled-lookback scan (per ensemble), the persistent particle kernel with one
+// packed 64-bit atomicMin per particle, the splat-parallel validation path, and resolve.
+//
+// Arithmetic follows shaders/gps_splat.wgsl expression by expression (left-to-right, IEEE f32,
+// no contraction: this file is compiled with --fmad=false) with the deterministic
+// transcendentals of fmath.h, so results are bit-identical to the CPU mirror oracle.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+#include "devmath.cuh"
+
+namespace gpsb {
+
+typedef unsigned long long ull;
+
+// ============================================================================ geometry
+// Once per camera: projection, opacity clamp, per-method count descriptor and particle record,
+// and the view-dependent SH colour (prepare/prepare_gps/prepare_pbvr without the seed-dependent
+// Poisson draw, gps_splat.wgsl:535-642; splat_colour :210-251).
+__global__ void __launch_bounds__(128) k_geometry(FrameConst f, const float4* __restrict__ splats,
+                                                   const float* __restrict__ sh, float4* __restrict__ rec,
+                                                   uint2* __restrict__ cdesc, float4* __restrict__ colour) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= f.N) return;
+    float4 g0 = __ldg(&splats[4 * (size_t)i]);
+    float4 g1 = __ldg(&splats[4 * (size_t)i + 1]);
+    float4 g2 = __ldg(&splats[4 * (size_t)i + 2]);
+    float4 g3 = __ldg(&splats[4 * (size_t)i + 3]);
+    uint2 cd = make_uint2(0u, CD_NONE);
+    Proj pr = project(f, g0, g1, g2);
+    float o = clamp_(g0.w, F_(0.0), F_(1.0));
+    float4* R = rec + (size_t)i * kRecF4;
+    if (pr.ok && o > F_(0.0)) {
+        float l00 = sqrt_(fmax_(pr.a, F_(1e-30)));
+        float l10 = div_(pr.b, l00);
+        float l11 = sqrt_(fmax_(pr.c - l10 * l10, F_(1e-30)));
+        float4 r0 = make_float4(pr.mx, pr.my, pr.depth, o);
+        const uint32_t method = f.method;
+        const float S = (float)f.S;
+        if (method == 0u) {
+            float ex = gxc::kOffscreenSigma * sqrt_(pr.a), ey = gxc::kOffscreenSigma * sqrt_(pr.c);
+            bool off = pr.mx + ex < F_(0.0) || pr.mx - ex >= (float)f.W || pr.my + ey < F_(0.0) || pr.my - ey >= (float)f.H;
+            if (!off) {
+                float det = pr.a * pr.c - pr.b * pr.b;
+                float li2 = dilog(o);
+                float en = f.density * S * F_(2.0) * gxc::kPi * sqrt_(det) * li2;
+                if (en > F_(0.0)) cd = make_uint2(f2b(en), CD_POISSON_CAP);
+                float fo = (F_(1.0) - sqrt_(fmax_(F_(1.0) - fmin_(o, F_(1.0)), F_(0.0)))) * F_(64.0);
+                uint32_t i0 = min(f2u(fo), 63u);
+                float a = fo - (float)i0;
+                R[0] = r0;
+                R[1] = make_float4(l00, l10, l11, a);
+                R[2] = make_float4(__uint_as_float(i0), li2, F_(0.0), F_(0.0));
+            }
+        } else if (method == 4u) {
+            float density = fmax_(f.density, F_(1e-8));
+            float amin = fmax_(F_(1.0) - gx::exp(div_(gxc::kLn254over255, density)), F_(1e-8));
+            if (o > amin) {
+                float radius = sqrt_(F_(2.0) * gx::log(div_(o, amin)));
+                float ext_x = radius * sqrt_(pr.a), ext_y = radius * sqrt_(pr.c);
+                float lo_x = clamp_(floorf(pr.mx - ext_x), F_(0.0), (float)f.W);
+                float lo_y = clamp_(floorf(pr.my - ext_y), F_(0.0), (float)f.H);
+                float hi_x = clamp_(ceilf(pr.mx + ext_x), F_(0.0), (float)f.W);
+                float hi_y = clamp_(ceilf(pr.my + ext_y), F_(0.0), (float)f.H);
+                float sz_x = fmax_(hi_x - lo_x, F_(0.0)), sz_y = fmax_(hi_y - lo_y, F_(0.0));
+                uint32_t count = f2u(sz_x) * f2u(sz_y) * f.side * f.side;
+                if (count != 0u) {
+                    float invdet = div_(F_(1.0), fmax_(pr.a * pr.c - pr.b * pr.b, F_(1e-30)));
+                    float peak_tau = -gx::log(F_(1.0) - fmin_(o, gxc::kOneMinus1e6));
+                    bool sparse = density * peak_tau < F_(1.0);
+                    if (sparse) cd = make_uint2(f2b((float)count * density * peak_tau), CD_POISSON);
+                    else cd = make_uint2(count, CD_FIXED);
+                    R[0] = r0;
+                    R[1] = make_float4(lo_x, lo_y, sz_x, sz_y);
+                    R[2] = make_float4(pr.c * invdet, -pr.b * invdet, pr.a * invdet, peak_tau);
+                    R[3] = make_float4(F_(0.0), F_(0.0), F_(0.0), sparse ? F_(1.0) : F_(0.0));
+                }
+            }
+        } else {
+            // pbvr_lambda (gps_splat.wgsl:441-460)
+            float g = extinction_term(o);
+            if (method == 1u) g = fmin_(o, gxc::kOneMinus1e6);
+            float scale = f.base_k;
+            if (method != 3u) {
+                uint32_t level = f.calibration;
+                if (level == 1u) scale = scale * pixel_density_scale(f, f.object_depth);
+                else if (level == 2u) scale = scale * pixel_density_scale(f, pr.depth);
+                else if (level == 3u) scale = S * F_(2.0) * gxc::kPi * sqrt_(pr.a * pr.c - pr.b * pr.b);
+            }
+            float lambda = f.density * g * scale;
+            if (!(lambda > F_(0.0)) || lambda > F_(3.0e38)) lambda = F_(0.0);
+            if (lambda > F_(0.0)) {
+                float det = pr.a * pr.c - pr.b * pr.b;
+                float keep = F_(1.0);
+                uint32_t flags = CD_POISSON_CAP;
+                if (method == 3u) {
+                    float target = f.density * S * F_(2.0) * gxc::kPi * sqrt_(det) * dilog(o);
+                    if (lambda > F_(0.5)) keep = clamp_(div_(target, lambda), F_(0.0), F_(1.0)); else keep = F_(0.0);
+                    if (target > lambda) flags |= CD_UNDERCOVERED;
+                }
+                cd = make_uint2(f2b(lambda), flags);
+                float idet = div_(F_(1.0), fmax_(det, F_(1e-30)));
+                // chol_of (gps_splat.wgsl:464-485)
+                float c0[3], c1[3], c2[3];
+                rot_cols(g2, c0, c1, c2);
+                float s2x = gx::exp(F_(2.0) * g1.x), s2y = gx::exp(F_(2.0) * g1.y), s2z = gx::exp(F_(2.0) * g1.z);
+                float a00 = s2x * c0[0] * c0[0] + s2y * c1[0] * c1[0] + s2z * c2[0] * c2[0];
+                float a10 = s2x * c0[1] * c0[0] + s2y * c1[1] * c1[0] + s2z * c2[1] * c2[0];
+                float a20 = s2x * c0[2] * c0[0] + s2y * c1[2] * c1[0] + s2z * c2[2] * c2[0];
+                float a11 = s2x * c0[1] * c0[1] + s2y * c1[1] * c1[1] + s2z * c2[1] * c2[1];
+                float a21 = s2x * c0[2] * c0[1] + s2y * c1[2] * c1[1] + s2z * c2[2] * c2[1];
+                float a22 = s2x * c0[2] * c0[2] + s2y * c1[2] * c1[2] + s2z * c2[2] * c2[2];
+                float k00 = sqrt_(fmax_(a00, F_(1e-30)));
+                float k10 = div_(a10, k00);
+                float k20 = div_(a20, k00);
+                float k11 = sqrt_(fmax_(a11 - k10 * k10, F_(1e-30)));
+                float k21 = div_(a21 - k20 * k10, k11);
+                float k22 = sqrt_(fmax_(a22 - k20 * k20 - k21 * k21, F_(1e-30)));
+                R[0] = r0;
+                R[1] = make_float4(keep, eol(fmin_(o, gxc::kOneMinus1e6)), F_(0.0), F_(0.0));
+                R[2] = make_float4(g0.x, g0.y, g0.z, pr.c * idet);
+                R[3] = make_float4(-pr.b * idet, pr.a * idet, F_(0.0), F_(0.0));
+                R[4] = make_float4(k00, k10, k11, F_(0.0));
+                R[5] = make_float4(k20, k21, k22, F_(0.0));
+            }
+        }
+    }
+    cdesc[i] = cd;
+    if ((cd.y & 3u) != CD_NONE) colour[i] = splat_colour(f, sh, i, g0, g3);
+}
+
+void launch_geometry(const FrameConst& fc, const float4* splats, const float* sh, const float* lut, float4* rec,
+                     uint2* cdesc, float4* colour, cudaStream_t st) {
+    (void)lut;
+    if (fc.N == 0) return;
+    k_geometry<<<(fc.N + 127) / 128, 128, 0, st>>>(fc, splats, sh, rec, cdesc, colour);
+}
+
+// ============================================================================ count + scan
+__device__ __forceinline__ uint64_t ld_relaxed(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t sat_add(uint64_t a, uint64_t b) {
+    uint64_t s = a + b;
+    return s > kLbSumSat ? kLbSumSat : s;
+}
+__device__ __forceinline__ uint64_t lb_pack(uint64_t status, uint64_t sum, uint32_t nz) {
+    return status | ((sum > kLbSumSat ? kLbSumSat : sum) << 24) | (uint64_t)nz;
+}
+
+// Per ensemble e and tile t of kScanTile splats: Poisson count of every splat with the stream
+// particle_seed(i, 0, first_seed + e) (gps_splat.wgsl:539-548, 593-602, 573-574), the per-splat cap,
+// the statistics of prepare, then a block scan and a decoupled lookback over the tiles of the
+// ensemble. Splats with a non-zero count are written, in splat order, to the compact list
+// clist[e * N + j] = (splat id, exclusive particle offset). The last tile writes the ensemble
+// total; a total above 2^32 - 1 marks the ensemble skipped (gps_splat.wgsl:635-639, 648-654).
+__global__ void __launch_bounds__(kScanThreads) k_count_scan(FrameConst f, const uint2* __restrict__ cdesc,
+                                                             uint32_t first_seed, uint32_t tiles_per_e,
+                                                             uint64_t* lookback, uint32_t* tile_counter,
+                                                             uint2* __restrict__ clist, EnsTotal* etot, ull* stats,
+                                                             uint32_t* err) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_wsum[kScanThreads / 32];
+    __shared__ uint32_t s_wnz[kScanThreads / 32];
+    __shared__ uint64_t s_excl_sum;
+    __shared__ uint32_t s_excl_nz;
+    __shared__ ull s_stat[6];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+    if (tid < 6) s_stat[tid] = 0ull;
+    __syncthreads();
+    const uint32_t id = s_tile;
+    const uint32_t e = id / tiles_per_e, t = id % tiles_per_e;
+    const uint32_t seed = first_seed + e;
+    const uint32_t N = f.N, cap = f.cap;
+    const bool gps = f.method == 0u;
+    const uint32_t base = t * kScanTile + tid * kScanItems;
+
+    uint32_t cnt[kScanItems];
+    ull st_pts = 0, st_trunc = 0, st_drop = 0, st_vis = 0, st_cand = 0, st_under = 0;
+    uint64_t tsum = 0;
+    uint32_t tnz = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        uint32_t i = base + q;
+        uint32_t n = 0;
+        if (i < N) {
+            uint2 cd = __ldg(&cdesc[i]);
+            uint32_t mode = cd.y & 3u;
+            if (mode == CD_FIXED) {
+                n = cd.x;
+                st_cand += n;
+                st_vis += 1;
+            } else if (mode != CD_NONE) {
+                uint32_t rs = gx::particle_seed(i, 0u, seed);
+                n = poisson(__uint_as_float(cd.x), &rs);
+                if (gps) st_pts += n; else st_cand += n;
+                st_vis += 1;
+                if (mode == CD_POISSON_CAP && n > cap) {
+                    st_trunc += 1;
+                    st_drop += n - cap;
+                    n = cap;
+                }
+            }
+            if (cd.y & CD_UNDERCOVERED) st_under += 1;
+        }
+        cnt[q] = n;
+        tsum += n;
+        tnz += n ? 1u : 0u;
+    }
+    // statistics: warp reduce, then shared, then one atomic per non-zero word per block
+    ull sv[6] = {st_pts, st_trunc, st_drop, st_vis, st_cand, st_under};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        ull v = sv[k];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(&s_stat[k], v);
+    }
+    // block scan of (tsum, tnz)
+    uint64_t isum = tsum;
+    uint32_t inz = tnz;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t a = __shfl_up_sync(0xffffffffu, isum, o);
+        uint32_t b = __shfl_up_sync(0xffffffffu, inz, o);
+        if (lane >= o) { isum += a; inz += b; }
+    }
+    if (lane == 31) { s_wsum[warp] = isum; s_wnz[warp] = inz; }
+    __syncthreads();
+    uint64_t wpre = 0;
+    uint32_t wpre_nz = 0, agg_nz = 0;
+    uint64_t agg = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w) {
+        if (w < warp) { wpre += s_wsum[w]; wpre_nz += s_wnz[w]; }
+        agg += s_wsum[w];
+        agg_nz += s_wnz[w];
+    }
+    // decoupled lookback over the tiles of ensemble e
+    uint64_t* lb = lookback + (size_t)e * tiles_per_e;
+    if (warp == 0) {
+        uint64_t excl = 0;
+        uint32_t excl_nz = 0;
+        if (t == 0) {
+            if (lane == 0) st_relaxed(&lb[0], lb_pack(kLbPrefix, agg, agg_nz));
+        } else {
+            if (lane == 0) st_relaxed(&lb[t], lb_pack(kLbAggregate, agg, agg_nz));
+            int32_t pred = (int32_t)t - 1;
+            uint32_t spins = 0;
+            bool failed = false;
+            while (true) {
+                int32_t j = pred - lane;
+                uint64_t w = 0;
+                if (j >= 0) {
+                    w = ld_relaxed(&lb[j]);
+                    while ((w >> 62) == 0ull) {
+                        if (++spins > (1u << 20)) { failed = true; break; }
+                        __nanosleep(64);
+                        w = ld_relaxed(&lb[j]);
+                    }
+                } else {
+                    w = kLbPrefix;  // before tile 0: an empty inclusive prefix
+                }
+                if (__any_sync(0xffffffffu, failed)) { failed = true; break; }
+                uint32_t is_prefix = __ballot_sync(0xffffffffu, (w >> 62) == 2ull);
+                int first = is_prefix ? __ffs(is_prefix) - 1 : 32;  // closest predecessor with a prefix
+                uint64_t v_sum = (lane <= first) ? ((w >> 24) & kLbSumSat) : 0ull;
+                uint32_t v_nz = (lane <= first) ? (uint32_t)(w & 0xFFFFFFull) : 0u;
+                for (int o = 16; o; o >>= 1) {
+                    v_sum += __shfl_xor_sync(0xffffffffu, v_sum, o);
+                    v_nz += __shfl_xor_sync(0xffffffffu, v_nz, o);
+                }
+                excl = sat_add(excl, v_sum);
+                excl_nz += v_nz;
+                if (first < 32) break;
+                pred -= 32;
+            }
+            if (failed) {
+                if (lane == 0) {
+                    atomicOr(err, ERR_SCAN_LOOKBACK);
+                    atomicOr(&etot[e].flags, 2u);
+                }
+                excl = 0;
+                excl_nz = 0;
+            }
+            if (lane == 0) st_relaxed(&lb[t], lb_pack(kLbPrefix, sat_add(excl, agg), excl_nz + agg_nz));
+        }
+        if (lane == 0) { s_excl_sum = excl; s_excl_nz = excl_nz; }
+    }
+    __syncthreads();
+    // compact list of non-zero splats
+    uint64_t off = s_excl_sum + wpre + (isum - tsum);
+    uint32_t j = s_excl_nz + wpre_nz + (inz - tnz);
+    uint2* out = clist + (size_t)e * N;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        if (cnt[q]) {
+            out[j] = make_uint2(base + q, (uint32_t)off);
+            off += cnt[q];
+            ++j;
+        }
+    }
+    if (tid < 6 && s_stat[tid]) {
+        const int word[6] = {ST_POINTS, ST_TRUNCATED, ST_DROPPED, ST_VISIBLE, ST_CANDIDATES, ST_UNDERCOVERED};
+        atomicAdd(&stats[word[tid]], s_stat[tid]);
+    }
+    if (t == tiles_per_e - 1 && tid == 0) {
+        uint64_t total = sat_add(s_excl_sum, agg);
+        etot[e].particles = total;
+        etot[e].nonzero = s_excl_nz + agg_nz;
+        if (total > 0xFFFFFFFFull) {
+            atomicOr(&etot[e].flags, 1u);
+            atomicAdd(&stats[ST_SKIPPED], 1ull);
+        }
+    }
+}
+
+void launch_count_scan(const FrameConst& fc, const uint2* cdesc, uint32_t first_seed, uint32_t E, uint64_t* lookback,
+                       uint32_t* tile_counter, uint2* clist, EnsTotal* etot, unsigned long long* stats, uint32_t* err,
+                       cudaStream_t st) {
+    uint32_t tiles = (fc.N + kScanTile - 1) / kScanTile;
+    cudaMemsetAsync(lookback, 0, (size_t)E * tiles * sizeof(uint64_t), st);
+    cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(etot, 0, (size_t)E * sizeof(EnsTotal), st);
+    if (fc.N == 0 || E == 0) return;
+    k_count_scan<<<tiles * E, kScanThreads, 0, st>>>(fc, cdesc, first_seed, tiles, lookback, tile_counter, clist, etot,
+                                                      stats, err);
+}
+
+// ============================================================================ particles
+constexpr int kLutN = 65 * 129;
+
+__device__ __forceinline__ void splat_write(ull* sub, uint32_t idx, float depth_z, uint32_t id) {
+    ull packed = ((ull)(f2b(depth_z) | 0x80000000u) << 32) | (ull)id;
+    ull cur = __ldcg(sub + idx);
+    if (packed < cur) atomicMin(sub + idx, packed);
+}
+
+// emit_particle (gps_splat.wgsl:259-282) with the packed winner rule
+__device__ __forceinline__ void emit_gps(const FrameConst& f, const float* lut, uint32_t i, uint32_t& rs, float4 r0,
+                                         float4 r1, float4 r2, ull* sub) {
+    float u = gx::next_u(&rs);
+    float r = f.exact_radius ? corrected_radius_exact(r0.w, r2.y, u) : corrected_radius_lut(lut, __float_as_uint(r2.x), r1.w, u);
+    float th = gxc::kTwoPi * gx::next_u(&rs);
+    float sn, cs;
+    gx::sincos(th, &sn, &cs);
+    float wx = r * cs, wy = r * sn;
+    float px_ = r0.x + r1.x * wx;
+    float py_ = r0.y + (r1.y * wx + r1.z * wy);
+    if (px_ < F_(0.0) || px_ >= (float)f.W || py_ < F_(0.0) || py_ >= (float)f.H) return;
+    uint32_t px = f2u(px_), py = f2u(py_);
+    uint32_t sx = min(f.side - 1u, f2u((px_ - (float)px) * (float)f.side));
+    uint32_t sy = min(f.side - 1u, f2u((py_ - (float)py) * (float)f.side));
+    splat_write(sub, (py * f.W + px) * f.S + sy * f.side + sx, r0.z, i);
+}
+
+struct Normal {
+    uint32_t* st;
+    bool has;
+    float spare;
+    __device__ __forceinline__ float next() {
+        if (has) { has = false; return spare; }
+        float u1 = fmax_(gx::next_u(st), gxc::kUMin);
+        float u2 = gx::next_u(st);
+        float r = sqrt_(-F_(2.0) * gx::log(u1));
+        float sn, cs;
+        gx::sincos(gxc::kTwoPi * u2, &sn, &cs);
+        spare = r * sn;
+        has = true;
+        return r * cs;
+    }
+};
+
+// emit_particle_pbvr (gps_splat.wgsl:490-532); returns 1 when the particle counts as a point
+__device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, uint32_t i, uint32_t& rs, const float4* R, ull* sub) {
+    Normal nm{&rs, false, F_(0.0)};
+    float uz = nm.next();
+    float uy = nm.next();
+    float ux = nm.next();
+    float4 r1 = R[1];
+    if (f.method == 3u) {
+        if (gx::next_u(&rs) >= r1.x) return 0u;
+    }
+    float4 r2 = R[2], r4 = R[4], r5 = R[5];
+    float wx = r2.x + r4.x * ux;
+    float wy = r2.y + (r4.y * ux + r4.z * uy);
+    float wz = r2.z + (r5.x * ux + r5.y * uy + r5.z * uz);
+    float px = wx - f.pos[0], py = wy - f.pos[1], pz = wz - f.pos[2];
+    float cx = dot3(f.rot0[0], f.rot0[1], f.rot0[2], px, py, pz);
+    float cy = dot3(f.rot1[0], f.rot1[1], f.rot1[2], px, py, pz);
+    float cz = dot3(f.rot2[0], f.rot2[1], f.rot2[2], px, py, pz);
+    if (cz <= f.near_z) return 0u;
+    float pix_x = div_(f.fx * cx, cz) + f.cx;
+    float pix_y = div_(f.fy * cy, cz) + f.cy;
+    const uint32_t flags = f.flags;
+    if (flags & FLAG_JITTER) {
+        float jy = nm.next();
+        float jx = nm.next();
+        float sj = sqrt_(fmax_(f.low_pass, F_(0.0)));
+        pix_x = pix_x + sj * jx;
+        pix_y = pix_y + sj * jy;
+    }
+    float4 r0 = R[0];
+    if (flags & FLAG_RADIAL) {
+        float4 r3 = R[3];
+        float dvx = pix_x - r0.x, dvy = pix_y - r0.y;
+        float r2v = r2.w * dvx * dvx + F_(2.0) * r3.x * dvx * dvy + r3.y * dvy * dvy;
+        // radial_keep (gps_splat.wgsl:434-438) with h(min(o, 1-1e-6)) hoisted per splat
+        float oo = fmin_(r0.w, gxc::kOneMinus1e6);
+        float y = oo * gx::exp(-F_(0.5) * fmax_(r2v, F_(0.0)));
+        float keep = clamp_(div_(eol(y), r1.y), F_(0.0), F_(1.0));
+        if (gx::next_u(&rs) >= keep) return 0u;
+    }
+    float depth_z = (flags & FLAG_CENTRE) ? r0.z : cz;
+    if (pix_x < F_(0.0) || pix_x >= (float)f.W || pix_y < F_(0.0) || pix_y >= (float)f.H) return 1u;
+    uint32_t ipx = f2u(pix_x), ipy = f2u(pix_y);
+    uint32_t sx = min(f.side - 1u, f2u((pix_x - (float)ipx) * (float)f.side));
+    uint32_t sy = min(f.side - 1u, f2u((pix_y - (float)ipy) * (float)f.side));
+    splat_write(sub, (ipy * f.W + ipx) * f.S + sy * f.side + sx, depth_z, i);
+    return 1u;
+}
+
+// ScreenOccupancy branch of particle_pass (gps_splat.wgsl:686-708); returns 1 on a hit
+__device__ __forceinline__ uint32_t emit_so(const FrameConst& f, uint32_t i, uint32_t k, uint32_t& rs, const float4* R,
+                                            ull* sub) {
+    float4 r0 = R[0], b = R[1];
+    const uint32_t side = f.side, samples = f.S;
+    bool sparse = R[3].w > F_(0.0);
+    uint32_t cell = k;
+    uint32_t bz = f2u(b.z), bw = f2u(b.w);
+    if (sparse) cell = min(f2u(gx::next_u(&rs) * b.z * b.w * (float)samples), bz * bw * samples - 1u);
+    uint32_t pixel = cell / samples, sub_i = cell % samples;
+    uint32_t xx = f2u(b.x) + pixel % bz, yy = f2u(b.y) + pixel / bz;
+    float n1 = gx::next_u(&rs);
+    float n2 = gx::next_u(&rs);
+    float uvx = div_((float)(sub_i % side) + n1, (float)side);
+    float uvy = div_((float)(sub_i / side) + n2, (float)side);
+    float dx = (float)xx + uvx - r0.x, dy = (float)yy + uvy - r0.y;
+    float4 inv = R[2];
+    float r2 = fmax_(inv.x * dx * dx + F_(2.0) * inv.y * dx * dy + inv.z * dy * dy, F_(0.0));
+    float alpha = fmin_(r0.w * gx::exp(-F_(0.5) * r2), gxc::kOneMinus1e6);
+    float coverage;
+    if (sparse) coverage = div_(-gx::log(F_(1.0) - alpha), inv.w);
+    else coverage = F_(1.0) - gx::exp(f.density * gx::log(F_(1.0) - alpha));
+    if (gx::next_u(&rs) >= coverage) return 0u;
+    splat_write(sub, (yy * f.W + xx) * samples + sub_i, r0.z, i);
+    return 1u;
+}
+
+constexpr int kPT = 256;               // threads per particle block
+constexpr int kPIPT = 8;               // particles per thread per tile
+constexpr int kPTile = kPT * kPIPT;    // particles per tile
+constexpr int kMaxE = 1024;            // ensembles per batch (shared prefix table)
+
+// Largest j in [lo, hi) with off(j) <= v, by a 32-ary warp search (off(lo) <= v must hold).
+__device__ __forceinline__ uint32_t warp_last_le(const uint2* __restrict__ L, uint32_t lo, uint32_t hi, uint64_t v, int lane) {
+    while (hi - lo > 1u) {
+        uint32_t n = hi - lo;
+        uint32_t step = (n + 31u) / 32u;
+        uint32_t idx = lo + (uint32_t)(lane + 1) * step;
+        bool p = idx < hi && (uint64_t)__ldg(&L[idx].y) <= v;
+        uint32_t c = __popc(__ballot_sync(0xffffffffu, p));
+        uint32_t nlo = lo + c * step;
+        uint32_t nhi = lo + (c + 1u) * step;
+        lo = nlo;
+        hi = nhi < hi ? nhi : hi;
+    }
+    return lo;
+}
+
+// Persistent particle kernel: every block repeatedly takes a tile of kPTile consecutive
+// particles of one ensemble (dynamic work counter), maps each particle to (splat i, k) through
+// the compact list, regenerates it from its own stream particle_seed(i, k + 1, seed) and writes it
+// with one 64-bit atomicMin of (depth key << 32 | i), which equals the reference's depth pass
+// followed by the colour pass (gps_splat.wgsl:276-281). Ensembles flagged skipped get no work.
+template <int MC>  // 0 GPS, 1 PBVR, 2 ScreenOccupancy
+__global__ void __launch_bounds__(kPT) k_particles(FrameConst f, const float4* __restrict__ rec,
+                                                   const float* __restrict__ lut, const uint2* __restrict__ clist,
+                                                   const EnsTotal* __restrict__ etot, uint32_t first_seed, uint32_t E,
+                                                   ull* sub, uint32_t* unit_counter, ull* stats) {
+    extern __shared__ float s_lut[];  // kLutN floats when GPS with the table radius
+    __shared__ uint64_t s_ubase[kMaxE + 1];
+    __shared__ uint32_t s_off[kPTile + 2];
+    __shared__ uint32_t s_id[kPTile + 2];
+    __shared__ uint32_t s_unit, s_j0, s_w;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const bool use_lut = MC == 0 && !f.exact_radius;
+    if (use_lut)
+        for (int k = tid; k < kLutN; k += kPT) s_lut[k] = __ldg(&lut[k]);
+    if (tid == 0) {
+        uint64_t acc = 0;
+        for (uint32_t e = 0; e < E; ++e) {
+            s_ubase[e] = acc;
+            EnsTotal t = etot[e];
+            if (t.flags == 0u && t.particles) acc += (t.particles + kPTile - 1) / kPTile;
+        }
+        s_ubase[E] = acc;
+    }
+    __syncthreads();
+    const uint64_t total_units = s_ubase[E];
+    const uint64_t PS = (uint64_t)f.W * f.H * f.S;
+    uint32_t points = 0;
+    for (;;) {
+        if (tid == 0) s_unit = atomicAdd(unit_counter, 1u);
+        __syncthreads();
+        const uint64_t u = s_unit;
+        if (u >= total_units) break;
+        // ensemble of unit u: largest e with s_ubase[e] <= u
+        uint32_t lo = 0, hi = E;
+        while (hi - lo > 1u) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (s_ubase[mid] <= u) lo = mid; else hi = mid;
+        }
+        const uint32_t e = lo;
+        const EnsTotal et = etot[e];
+        const uint64_t p0 = (u - s_ubase[e]) * kPTile;
+        const uint64_t p1 = p0 + kPTile < et.particles ? p0 + kPTile : et.particles;
+        const uint2* L = clist + (size_t)e * f.N;
+        if (tid < 32) {
+            uint32_t j0 = warp_last_le(L, 0u, et.nonzero, p0, lane);
+            uint32_t j1 = warp_last_le(L, j0, et.nonzero, p1 - 1, lane);
+            if (lane == 0) { s_j0 = j0; s_w = j1 - j0 + 1u; }
+        }
+        __syncthreads();
+        const uint32_t j0 = s_j0, w = s_w;
+        for (uint32_t q = tid; q <= w; q += kPT) {
+            uint32_t j = j0 + q;
+            if (q < w) {
+                uint2 ent = __ldg(&L[j]);
+                s_id[q] = ent.x;
+                s_off[q] = ent.y;
+            } else {
+                s_off[q] = j < et.nonzero ? __ldg(&L[j].y) : (uint32_t)et.particles;
+            }
+        }
+        __syncthreads();
+        const uint32_t seed = first_seed + e;
+        ull* S = sub + (size_t)e * PS;
+        uint64_t p = p0 + (uint64_t)tid * kPIPT;
+        if (p < p1) {
+            uint32_t pp = (uint32_t)p;
+            // entry of particle pp in the window
+            uint32_t a = 0, b = w;
+            while (b - a > 1u) {
+                uint32_t m = (a + b) >> 1;
+                if (s_off[m] <= pp) a = m; else b = m;
+            }
+            uint32_t jj = a;
+            uint32_t cur = 0xFFFFFFFFu;
+            float4 R[kRecF4];
+            const uint32_t pend = (uint32_t)(p + kPIPT < p1 ? p + kPIPT : p1);
+            for (; pp < pend; ++pp) {
+                while (pp >= s_off[jj + 1]) ++jj;
+                const uint32_t i = s_id[jj];
+                const uint32_t k = pp - s_off[jj];
+                if (i != cur) {
+                    cur = i;
+                    const float4* Rg = rec + (size_t)i * kRecF4;
+                    R[0] = __ldg(&Rg[0]);
+                    R[1] = __ldg(&Rg[1]);
+                    if (MC != 1) R[2] = __ldg(&Rg[2]);
+                    if (MC == 1) {
+                        R[2] = __ldg(&Rg[2]);
+                        R[3] = __ldg(&Rg[3]);
+                        R[4] = __ldg(&Rg[4]);
+                        R[5] = __ldg(&Rg[5]);
+                    }
+                    if (MC == 2) R[3] = __ldg(&Rg[3]);
+                }
+                uint32_t rs = gx::particle_seed(i, k + 1u, seed);
+                if (MC == 0) emit_gps(f, s_lut, i, rs, R[0], R[1], R[2], S);
+                else if (MC == 1) points += emit_pbvr(f, i, rs, R, S);
+                else points += emit_so(f, i, k, rs, R, S);
+            }
+        }
+        __syncthreads();
+    }
+    if (MC != 0) {
+        ull v = points;
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(&stats[ST_POINTS], v);
+    }
+}
+
+void launch_particles(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
+                      const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
+                      uint32_t* unit_counter, unsigned long long* stats, int grid, cudaStream_t st) {
+    cudaMemsetAsync(unit_counter, 0, sizeof(uint32_t), st);
+    if (fc.N == 0 || E == 0) return;
+    if (fc.method == 0u) {
+        size_t smem = fc.exact_radius ? 0 : kLutN * sizeof(float);
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaFuncSetAttribute(k_particles<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kLutN * sizeof(float)));
+            attr_set = true;
+        }
+        k_particles<0><<<grid, kPT, smem, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
+    } else if (fc.method == 4u) {
+        k_particles<2><<<grid, kPT, 0, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
+    } else {
+        k_particles<1><<<grid, kPT, 0, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
+    }
+}
+
+// ============================================================================ primitive path
+// splat_pass (gps_splat.wgsl:304-333): one thread per splat and ensemble generates all particles
+// of the splat from one sequential stream. Validation path of GPS only (RenderPath::Primitive).
+__global__ void __launch_bounds__(128) k_primitive(FrameConst f, const float4* __restrict__ rec,
+                                                   const uint2* __restrict__ cdesc, const float* __restrict__ lut,
+                                                   uint32_t first_seed, uint32_t E, ull* sub, ull* stats) {
+    uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = gi % f.N, e = gi / f.N;
+    if (e >= E) return;
+    uint2 cd = __ldg(&cdesc[i]);
+    if ((cd.y & 3u) != CD_POISSON_CAP) return;
+    uint32_t rs = gx::particle_seed(i, 0u, first_seed + e);
+    uint32_t n = poisson(__uint_as_float(cd.x), &rs);
+    atomicAdd(&stats[ST_POINTS], (ull)n);
+    atomicAdd(&stats[ST_VISIBLE], 1ull);
+    if (n > f.cap) {
+        atomicAdd(&stats[ST_TRUNCATED], 1ull);
+        atomicAdd(&stats[ST_DROPPED], (ull)(n - f.cap));
+        n = f.cap;
+    }
+    const float4* Rg = rec + (size_t)i * kRecF4;
+    float4 r0 = Rg[0], r1 = Rg[1], r2 = Rg[2];
+    ull* S = sub + (size_t)e * ((uint64_t)f.W * f.H * f.S);
+    for (uint32_t q = 0; q < n; ++q) emit_gps(f, lut, i, rs, r0, r1, r2, S);
+}
+
+void launch_primitive(const FrameConst& fc, const float4* rec, const uint2* cdesc, const float* lut,
+                      uint32_t first_seed, uint32_t E, unsigned long long* sub, EnsTotal* etot,
+                      unsigned long long* stats, cudaStream_t st) {
+    cudaMemsetAsync(etot, 0, (size_t)E * sizeof(EnsTotal), st);
+    if (fc.N == 0 || E == 0) return;
+    uint64_t n = (uint64_t)fc.N * E;
+    k_primitive<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(fc, rec, cdesc, lut, first_seed, E, sub, stats);
+}
+
+// ============================================================================ resolve
+// resolve (gps_splat.wgsl:362-386) for every ensemble of the batch, in ensemble order, so the
+// f32 accumulation sequence equals the reference's one resolve per ensemble.
+__global__ void __launch_bounds__(256) k_resolve(FrameConst f, const ull* __restrict__ sub,
+                                                  const EnsTotal* __restrict__ etot, const float4* __restrict__ colour,
+                                                  uint32_t E, float4* accum, ull* stats) {
+    uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t P = f.W * f.H;
+    if (pix >= P) return;
+    const uint32_t S = f.S;
+    const uint64_t PS = (uint64_t)P * S;
+    float4 acc = accum[pix];
+    const float inv_bg0 = f.bg[0], inv_bg1 = f.bg[1], inv_bg2 = f.bg[2];
+    uint32_t orphans = 0;
+    for (uint32_t e = 0; e < E; ++e) {
+        if (__ldg(&etot[e].flags) != 0u) continue;
+        const ull* s = sub + (size_t)e * PS + (size_t)pix * S;
+        float sx = F_(0.0), sy = F_(0.0), sz = F_(0.0);
+        for (uint32_t k = 0; k < S; ++k) {
+            ull v = __ldcs(s + k);
+            uint32_t key = (uint32_t)(v >> 32), id = (uint32_t)v;
+            if (key == gxc::kEmpty) {
+                sx = sx + inv_bg0; sy = sy + inv_bg1; sz = sz + inv_bg2;
+            } else if (id == gxc::kEmpty) {
+                ++orphans;
+                sx = sx + inv_bg0; sy = sy + inv_bg1; sz = sz + inv_bg2;
+            } else {
+                float4 c = __ldg(&colour[id]);
+                sx = sx + c.x; sy = sy + c.y; sz = sz + c.z;
+            }
+        }
+        const float Sf = (float)S;
+        acc.x = acc.x + div_(sx, Sf);
+        acc.y = acc.y + div_(sy, Sf);
+        acc.z = acc.z + div_(sz, Sf);
+        acc.w = acc.w + F_(1.0);
+    }
+    accum[pix] = acc;
+    if (orphans) atomicAdd(&stats[ST_ORPHAN], (ull)orphans);
+}
+
+void launch_resolve(const FrameConst& fc, const unsigned long long* sub, const EnsTotal* etot, const float4* colour,
+                    uint32_t E, float4* accum, unsigned long long* stats, cudaStream_t st) {
+    uint32_t P = fc.W * fc.H;
+    if (P == 0 || E == 0) return;
+    k_resolve<<<(P + 255) / 256, 256, 0, st>>>(fc, sub, etot, colour, E, accum, stats);
+}
+
+__global__ void k_add_stat(ull* stats, int word, ull v) { stats[word] += v; }
+void launch_add_stat(unsigned long long* stats, int word, unsigned long long v, cudaStream_t st) {
+    k_add_stat<<<1, 1, 0, st>>>(stats, word, v);
+}
+
+int device_sm_count(int device) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+    return n;
+}
+
+}  // namespace gpsb

@@ -230,6 +230,8 @@ uint32_t gpsb_debug_error_word(gpsb_renderer* r);
  * n*3*((d+1)^2-1) SH floats. */
 gpsb_status gpsb_load_ply(const uint8_t* bytes, size_t len, size_t* n_out, uint32_t* sh_degree_out,
                           gpsb_gaussian* splats, float* sh_rest);
+/* Message of the last gpsb_load_ply failure on this thread (PlyError's Display, gps-io lib.rs:29-46). */
+const char* gpsb_ply_last_error(void);
 
 #ifdef __cplusplus
 }
