@@ -1,0 +1,407 @@
+"""Benchmark of the stochastic particle-rendering path on B200.
+
+Workload: 560,000 synthetic Gaussians (64 anisotropic clusters + 10%
+background, SH degree 3), PBVR Extinction C3+R, spp 1, per-splat cap 16,384, 1280x720, 64
+ensembles at each of three orbit distances (near 2.5, mid 7, far 20). One step renders the 64
+ensembles of all three views (192 ensembles); the metric is whole-job ensembles per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank renders its own ensembles (seeds offset by
+rank) of the same views: weak scaling, no collective on the data path; the timed region is
+bracketed by a barrier + synchronize and the max over ranks is reported.
+`--impl reference` times the reference's CPU implementation of the path (the C++ port of
+gps-core's render_particles_3d, oracle/o1_core.cpp) on the host cores, on rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, SIDE, ENS, CAP, N_SPLATS = 1280, 720, 1, 64, 16384, 560_000
+VIEWS = (("near", 2.5), ("mid", 7.0), ("far", 20.0))
+
+
+def load_package():
+    import importlib.util
+    name = "gps_pbvr_web_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    d = os.path.join(ROOT, "gps-pbvr-web_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(d, "__init__.py"), submodule_search_locations=[d])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config():
+    return {"workload": "PBVR Extinction C3+R, 560k synthetic Gaussians (64 clusters + 10% background, SH3), "
+                        "1280x720 spp1, cap 16384, 64 ensembles x near/mid/far orbit (2.5/7/20)",
+            "gaussians": N_SPLATS, "resolution": [W, H], "spp_side": SIDE, "ensembles_per_view": ENS,
+            "views": [v for v, _ in VIEWS], "cap": CAP, "method": "PBVR Extinction C3+R", "sh_degree": 3,
+            "l2": "inputs larger than L2 (64 subpixel buffers = 472 MB per view, scene 136 MB)"}
+
+
+def build_scene(pkg):
+    from gps_pbvr_web_b200 import scenes
+    ply = scenes.cluster_scene(N_SPLATS, seed=0, degree=3)
+    return pkg.load_ply(ply)
+
+
+def params(pkg):
+    p = pkg.RenderParams(spp_side=SIDE, max_points_per_splat=CAP, method=pkg.Method.Extinction)
+    p.pbvr.calibration = pkg.Calibration.PerSplatFootprint
+    p.pbvr.radial_correction = True
+    return p
+
+
+def cameras(pkg, views=None):
+    out = []
+    for name, d in VIEWS:
+        if views and name not in views:
+            continue
+        cam = pkg.OrbitCamera(target=(0.0, 0.0, 0.0), distance=d, yaw=0.6, pitch=0.25, up=(0.0, -1.0, 0.0), fov_y=0.9)
+        out.append((name, cam.to_camera(W, H)))
+    return out
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.rows, self.proc = device, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        res = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows)}
+        if not self.rows:
+            return res
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        loaded = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        res["sm_mhz"] = statistics.median(loaded) if loaded else None
+        res["sm_max_mhz"] = max(mx) if mx else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for k, n in enumerate(names):
+            if any(r[4 + k].lower() == "active" for r in self.rows):
+                res["reasons"].append(n)
+        return res
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "of measured"
+    except Exception:
+        return 6650.0, "of fallback"
+
+
+def committed_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.md), or None."""
+    import re
+    path = os.path.join(ROOT, "profiles", "traffic.md")
+    try:
+        for line in open(path):
+            m = re.match(r"\|\s*(\S+)\s*\|\s*([0-9.eE+]+)\s*\|", line)
+            if m and m.group(1) == kernel:
+                return float(m.group(2))
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------------------ CPU reference
+def cpu_reference(pkg, splats, fraction, threads, views_cams, first_seed=1):
+    """O1 render_particles_3d (the C++ port of gps-core, with the GPU's per-splat cap) on the first
+    `fraction` of the splats (a uniform subset: the generator shuffles splats), one ensemble per
+    thread per view. Returns (ensembles/s scaled to the full scene, per-view ms/ensemble)."""
+    import oracle as O
+    n = max(1, int(len(splats) * fraction))
+    g = splats[:n]
+    sc = {"pos": g[:, 0:3].astype(np.float64), "log_scale": g[:, 4:7].astype(np.float64),
+          "rot_xyzw": np.concatenate([g[:, 9:12], g[:, 8:9]], axis=1).astype(np.float64),
+          "opacity": g[:, 3].astype(np.float64), "color": g[:, 12:15].astype(np.float64)}
+    per_view = {}
+    total_s_per_ens = 0.0
+    for name, cam in views_cams:
+        t = time.perf_counter()
+        O.render_particles_3d(sc, cam.to_array(), W, H, SIDE, threads, (0.05, 0.05, 0.08), first_seed, level=3, rule=1,
+                              radial_correction=True, per_particle_seed=True, threads=threads, max_points_per_splat=CAP)
+        dt = time.perf_counter() - t
+        s_per_ens = dt / threads / (n / len(splats))  # wall seconds per full-scene ensemble at `threads` in parallel
+        per_view[name] = 1000.0 * s_per_ens
+        total_s_per_ens += s_per_ens
+    return len(views_cams) / total_s_per_ens, per_view
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    pkg = load_package()
+    splats, sh, deg = build_scene(pkg)
+    cams = cameras(pkg)
+    threads = os.cpu_count() or 1
+    fraction = args.cpu_fraction
+    for _ in range(args.warmup):
+        cpu_reference(pkg, splats, fraction, threads, cams)
+    rates, views = [], []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r, v = cpu_reference(pkg, splats, fraction, threads, cams)
+        rates.append(r)
+        views.append(v)
+    wall = time.perf_counter() - t0
+    value = statistics.median(rates)
+    sample = (f"first {fraction:g} of the {N_SPLATS} splats (uniform subset), {threads} ensembles in parallel "
+              f"(one per thread) per view, time scaled to the full scene")
+    line = {"impl": "reference", "metric": "ensembles/s (PBVR Ext C3+R, 560k Gaussians SH3, 1280x720, near/mid/far)",
+            "value": value, "unit": "ensembles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * wall / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+            "ms_per_ensemble": {k: statistics.median([v[k] for v in views]) for k in views[0]},
+            "cpu_baseline": {"value": value, "unit": "ensembles/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "ensembles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------ GPU arm
+def algorithmic_bytes_per_launch(stage, writes, entries, E, n_splats, P):
+    """Bytes one launch of `stage` must move (the roofline basis, one view of E ensembles):
+    writes / entries = on-screen particle writes and compact-list entries of that launch."""
+    if stage == "particles":   # one 8-byte atomicMin per written particle, list entry + 96-byte record per entry
+        return 8.0 * writes + (8.0 + 96.0) * entries
+    if stage == "count_scan":  # 8-byte count descriptor per splat and ensemble, 8-byte list entry written
+        return 8.0 * n_splats * E + 8.0 * entries
+    if stage == "resolve":     # every subpixel word of every ensemble, accum read + write
+        return 8.0 * P * SIDE * SIDE * E + 32.0 * P
+    if stage == "clear":       # every subpixel word of every ensemble
+        return 8.0 * P * SIDE * SIDE * E
+    if stage == "geometry":    # splat + SH3 read, record + descriptor + colour written
+        return (64.0 + 180.0 + 96.0 + 8.0 + 16.0) * n_splats
+    return 0.0
+
+
+def run_b200(args, rank, world):
+    import torch
+    pkg = load_package()
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    splats, sh, deg = build_scene(pkg)
+    cams = cameras(pkg, args.views)
+    ENS = args.ensembles
+    p = params(pkg)
+    stream = torch.cuda.Stream(device=dev)
+    r = pkg.GpsRenderer(W, H, SIDE, device=dev)
+    r.set_stream(stream.cuda_stream)
+    r.set_gaussians_sh(splats, sh, deg)
+    seed0 = 1 + rank * 1_000_003
+
+    def step(seed):
+        for _, cam in cams:
+            r.reset_accum()
+            r.render_ensembles(cam, p, seed, ENS)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for k in range(args.warmup):
+        step(seed0)
+    torch.cuda.synchronize()
+    r.reset_stats()
+    r.profile_enable(True)
+    clocks = ClockSampler(dev)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        step(seed0)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = t_start.elapsed_time(t_end)
+    prof = r.profile()
+    st = r.read_stats()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ens_total = world * args.steps * len(cams) * ENS
+    value = ens_total / (ms / 1000.0)
+
+    # per-view breakdown (outside the timed region)
+    per_view = {}
+    for name, cam in cams:
+        r.reset_accum()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r.render_ensembles(cam, p, seed0, ENS)
+        b.record(stream)
+        torch.cuda.synchronize()
+        per_view[name] = a.elapsed_time(b) / ENS
+
+    # roofline of the dominant kernel: algorithmic bytes per launch / average launch duration
+    P = W * H
+    views_per_step = len(cams)
+    writes_pl = st.subpixel_writes / (args.steps * views_per_step)
+    entries_pl = st.list_entries / (args.steps * views_per_step)
+    stage = max(prof["ms"], key=lambda k: prof["ms"][k])
+    avg_launch_ms = prof["ms"][stage] / max(prof["launches"][stage], 1)
+    bytes_per_launch = algorithmic_bytes_per_launch(stage, writes_pl, entries_pl, ENS, len(splats), P)
+    achieved = bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9
+    peak, peak_kind = measured_peak()
+    kernel_name = {"particles": "k_particles", "count_scan": "k_count_scan", "resolve": "k_resolve",
+                   "geometry": "k_geometry", "clear": "memset"}.get(stage, stage)
+    traffic = committed_traffic(kernel_name)
+    stage_gbs = {}
+    for sname in ["particles", "count_scan", "resolve", "clear", "geometry"]:
+        if prof["launches"][sname]:
+            b = algorithmic_bytes_per_launch(sname, writes_pl, entries_pl, ENS, len(splats), P)
+            t_ms = prof["ms"][sname] / prof["launches"][sname]
+            stage_gbs[sname] = {"ms_per_launch": t_ms, "alg_GBps": b / (t_ms / 1000.0) / 1e9,
+                                "share": prof["ms"][sname] / max(sum(prof["ms"].values()), 1e-9)}
+
+    # end to end through the public API: host scene upload, render, host readback, every step
+    e2e = None
+    if not args.no_e2e:
+        pin_g = torch.from_numpy(splats.reshape(-1)).pin_memory()
+        pin_s = torch.from_numpy(sh).pin_memory()
+        out = torch.empty((P, 4), dtype=torch.float32).pin_memory()
+        L = pkg.abi.lib()
+        import ctypes as C
+        pc = p.to_c()
+        cc = [c.to_c() for _, c in cams]
+
+        def ok(status):
+            if status != 0:
+                raise RuntimeError(L.gpsb_last_error(r.handle).decode())
+
+        def e2e_step():
+            ok(L.gpsb_set_gaussians_sh(r.handle, C.c_void_p(pin_g.data_ptr()), len(splats),
+                                       C.c_void_p(pin_s.data_ptr()), pin_s.numel(), deg))
+            for c in cc:
+                ok(L.gpsb_reset_accum(r.handle))
+                ok(L.gpsb_render_ensembles(r.handle, C.byref(c), C.byref(pc), seed0, ENS))
+                ok(L.gpsb_read_accum(r.handle, C.c_void_p(out.data_ptr())))
+
+        e2e_step()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e_steps = max(1, min(args.steps, 5))
+        for _ in range(e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        e2e = {"value": world * e_steps * len(cams) * ENS / dt, "unit": "ensembles/s",
+               "h2d_bytes_per_step": int(splats.nbytes + sh.nbytes), "d2h_bytes_per_step": int(len(cams) * P * 16),
+               "steps": e_steps, "timing": "host wall clock around synchronised steps"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cams = cameras(pkg)
+        threads = os.cpu_count() or 1
+        rate, cpu_views = cpu_reference(pkg, splats, args.cpu_fraction, threads, cams)
+        cpu = {"value": rate, "unit": "ensembles/s", "cores": threads, "kind": "port",
+               "sample": f"first {args.cpu_fraction:g} of the {N_SPLATS} splats (uniform subset), one ensemble per "
+                         f"thread per view, {threads} threads, time scaled to the full scene",
+               "ms_per_ensemble": cpu_views}
+
+    if rank == 0:
+        line = {"metric": "ensembles/s (PBVR Ext C3+R, 560k Gaussians SH3, 1280x720, near/mid/far)",
+                "value": value, "unit": "ensembles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
+                "config": dict(workload_config(), views=[n for n, _ in cams], ensembles_per_view=ENS),
+                "ms_per_ensemble": per_view,
+                "particles_per_s": world * st.subpixel_writes / (ms / 1000.0) / 1.0,
+                "points_per_s": world * st.points / (ms / 1000.0),
+                "gaussians_per_s": world * args.steps * len(cams) * ENS * len(splats) / (ms / 1000.0),
+                "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak,
+                             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic},
+                "stages": stage_gbs, "clocks": clk, "gpu_launches": prof["total_launches"],
+                "stats_per_step": {"points": st.points / args.steps, "subpixel_writes": st.subpixel_writes / args.steps,
+                                   "list_entries": st.list_entries / args.steps,
+                                   "truncated_splats": st.truncated_splats / args.steps,
+                                   "skipped_ensembles": st.skipped_ensembles},
+                "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    r.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64)
+    ap.add_argument("--views", default="near,mid,far", help="subset of the views (small profiling cases)")
+    ap.add_argument("--ensembles", type=int, default=ENS, help="ensembles per view (small profiling cases)")
+    args = ap.parse_args()
+    args.views = [v for v in args.views.split(",") if v]
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_b200(args, rank, world)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -40,7 +40,15 @@ class StatsC(C.Structure):
     _fields_ = [("points", C.c_uint64), ("truncated_splats", C.c_uint64), ("dropped_points", C.c_uint64),
                 ("visible_splats", C.c_uint64), ("orphan_subpixels", C.c_uint64), ("candidates", C.c_uint64),
                 ("undercovered_splats", C.c_uint64), ("skipped_ensembles", C.c_uint64), ("ensembles", C.c_uint64),
-                ("probe_demand", C.c_uint64), ("issue", C.c_uint32), ("_pad", C.c_uint32)]
+                ("probe_demand", C.c_uint64), ("issue", C.c_uint32), ("_pad", C.c_uint32),
+                ("subpixel_writes", C.c_uint64), ("list_entries", C.c_uint64)]
+
+
+class ProfileC(C.Structure):
+    _fields_ = [("launches", C.c_uint64 * 8), ("ms", C.c_double * 8), ("total_launches", C.c_uint64)]
+
+
+STAGES = ["geometry", "count_scan", "particles", "resolve", "clear", "primitive", "sorted", "composite"]
 
 
 P = C.c_void_p
@@ -91,6 +99,8 @@ SIGNATURES = {
     "gpsb_debug_error_word": (U32, [P]),
     "gpsb_load_ply": (ST, [P, SZ, P, P, P, P]),
     "gpsb_ply_last_error": (C.c_char_p, []),
+    "gpsb_profile_enable": (ST, [P, C.c_int]),
+    "gpsb_profile_read": (ST, [P, P]),
 }
 
 _lib = None

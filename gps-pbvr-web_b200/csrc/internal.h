@@ -45,7 +45,8 @@ constexpr int kRecF4 = 6;
 // Statistics words (64-bit): gpsb_stats field order.
 enum : int {
     ST_POINTS = 0, ST_TRUNCATED = 1, ST_DROPPED = 2, ST_VISIBLE = 3, ST_ORPHAN = 4, ST_CANDIDATES = 5,
-    ST_UNDERCOVERED = 6, ST_SKIPPED = 7, ST_ENSEMBLES = 8, ST_PROBE = 9, ST_WORDS = 16
+    ST_UNDERCOVERED = 6, ST_SKIPPED = 7, ST_ENSEMBLES = 8, ST_PROBE = 9, ST_WRITES = 10, ST_ENTRIES = 11,
+    ST_WORDS = 16
 };
 
 // Device error word bits (bounded waits that gave up).

@@ -314,6 +314,7 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(FrameConst f, const
         uint64_t total = sat_add(s_excl_sum, agg);
         etot[e].particles = total;
         etot[e].nonzero = s_excl_nz + agg_nz;
+        atomicAdd(&stats[ST_ENTRIES], (ull)(s_excl_nz + agg_nz));
         if (total > 0xFFFFFFFFull) {
             atomicOr(&etot[e].flags, 1u);
             atomicAdd(&stats[ST_SKIPPED], 1ull);
@@ -343,8 +344,8 @@ __device__ __forceinline__ void splat_write(ull* sub, uint32_t idx, float depth_
 }
 
 // emit_particle (gps_splat.wgsl:259-282) with the packed winner rule
-__device__ __forceinline__ void emit_gps(const FrameConst& f, const float* lut, uint32_t i, uint32_t& rs, float4 r0,
-                                         float4 r1, float4 r2, ull* sub) {
+__device__ __forceinline__ uint32_t emit_gps(const FrameConst& f, const float* lut, uint32_t i, uint32_t& rs, float4 r0,
+                                             float4 r1, float4 r2, ull* sub) {
     float u = gx::next_u(&rs);
     float r = f.exact_radius ? corrected_radius_exact(r0.w, r2.y, u) : corrected_radius_lut(lut, __float_as_uint(r2.x), r1.w, u);
     float th = gxc::kTwoPi * gx::next_u(&rs);
@@ -353,11 +354,12 @@ __device__ __forceinline__ void emit_gps(const FrameConst& f, const float* lut, 
     float wx = r * cs, wy = r * sn;
     float px_ = r0.x + r1.x * wx;
     float py_ = r0.y + (r1.y * wx + r1.z * wy);
-    if (px_ < F_(0.0) || px_ >= (float)f.W || py_ < F_(0.0) || py_ >= (float)f.H) return;
+    if (px_ < F_(0.0) || px_ >= (float)f.W || py_ < F_(0.0) || py_ >= (float)f.H) return 0u;
     uint32_t px = f2u(px_), py = f2u(py_);
     uint32_t sx = min(f.side - 1u, f2u((px_ - (float)px) * (float)f.side));
     uint32_t sy = min(f.side - 1u, f2u((py_ - (float)py) * (float)f.side));
     splat_write(sub, (py * f.W + px) * f.S + sy * f.side + sx, r0.z, i);
+    return 1u;
 }
 
 struct Normal {
@@ -377,7 +379,7 @@ struct Normal {
     }
 };
 
-// emit_particle_pbvr (gps_splat.wgsl:490-532); returns 1 when the particle counts as a point
+// emit_particle_pbvr (gps_splat.wgsl:490-532); returns bit 0 = counts as a point, bit 1 = written
 __device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, uint32_t i, uint32_t& rs, const float4* R, ull* sub) {
     Normal nm{&rs, false, F_(0.0)};
     float uz = nm.next();
@@ -423,7 +425,7 @@ __device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, uint32_t i, u
     uint32_t sx = min(f.side - 1u, f2u((pix_x - (float)ipx) * (float)f.side));
     uint32_t sy = min(f.side - 1u, f2u((pix_y - (float)ipy) * (float)f.side));
     splat_write(sub, (ipy * f.W + ipx) * f.S + sy * f.side + sx, depth_z, i);
-    return 1u;
+    return 3u;
 }
 
 // ScreenOccupancy branch of particle_pass (gps_splat.wgsl:686-708); returns 1 on a hit
@@ -505,7 +507,7 @@ __global__ void __launch_bounds__(kPT) k_particles(FrameConst f, const float4* _
     __syncthreads();
     const uint64_t total_units = s_ubase[E];
     const uint64_t PS = (uint64_t)f.W * f.H * f.S;
-    uint32_t points = 0;
+    uint32_t points = 0, writes = 0;
     for (;;) {
         if (tid == 0) s_unit = atomicAdd(unit_counter, 1u);
         __syncthreads();
@@ -574,18 +576,28 @@ __global__ void __launch_bounds__(kPT) k_particles(FrameConst f, const float4* _
                     if (MC == 2) R[3] = __ldg(&Rg[3]);
                 }
                 uint32_t rs = gx::particle_seed(i, k + 1u, seed);
-                if (MC == 0) emit_gps(f, s_lut, i, rs, R[0], R[1], R[2], S);
-                else if (MC == 1) points += emit_pbvr(f, i, rs, R, S);
-                else points += emit_so(f, i, k, rs, R, S);
+                if (MC == 0) {
+                    writes += emit_gps(f, s_lut, i, rs, R[0], R[1], R[2], S);
+                } else if (MC == 1) {
+                    uint32_t r = emit_pbvr(f, i, rs, R, S);
+                    points += r & 1u;
+                    writes += r >> 1;
+                } else {
+                    uint32_t r = emit_so(f, i, k, rs, R, S);
+                    points += r;
+                    writes += r;
+                }
             }
         }
         __syncthreads();
     }
-    if (MC != 0) {
-        ull v = points;
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0 && v) atomicAdd(&stats[ST_POINTS], v);
+    ull v = points, wv = writes;
+    for (int o = 16; o; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+        wv += __shfl_xor_sync(0xffffffffu, wv, o);
     }
+    if (lane == 0 && v && MC != 0) atomicAdd(&stats[ST_POINTS], v);
+    if (lane == 0 && wv) atomicAdd(&stats[ST_WRITES], wv);
 }
 
 void launch_particles(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
@@ -631,7 +643,9 @@ __global__ void __launch_bounds__(128) k_primitive(FrameConst f, const float4* _
     const float4* Rg = rec + (size_t)i * kRecF4;
     float4 r0 = Rg[0], r1 = Rg[1], r2 = Rg[2];
     ull* S = sub + (size_t)e * ((uint64_t)f.W * f.H * f.S);
-    for (uint32_t q = 0; q < n; ++q) emit_gps(f, lut, i, rs, r0, r1, r2, S);
+    ull writes = 0;
+    for (uint32_t q = 0; q < n; ++q) writes += emit_gps(f, lut, i, rs, r0, r1, r2, S);
+    if (writes) atomicAdd(&stats[ST_WRITES], writes);
 }
 
 void launch_primitive(const FrameConst& fc, const float4* rec, const uint2* cdesc, const float* lut,

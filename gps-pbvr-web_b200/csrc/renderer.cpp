@@ -81,6 +81,49 @@ struct gpsb_renderer {
     uint32_t stats_issued = 0;
     gpsb_stats latest{};
     std::string error;
+    // profiling: CUDA-event pairs per stage, resolved at gpsb_profile_read
+    bool prof_on = false;
+    struct Pending { int stage; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    uint64_t launches[GPSB_STAGES] = {};
+    double ms[GPSB_STAGES] = {};
+    uint64_t total_launches = 0;
+};
+
+// Brackets the kernels of one stage with CUDA events on the renderer's stream (when profiling)
+// and counts the kernels launched.
+struct StageScope {
+    gpsb_renderer* r;
+    int stage;
+    cudaEvent_t a = nullptr;
+    StageScope(gpsb_renderer* rr, int st) : r(rr), stage(st) {
+        if (r->prof_on) {
+            a = take();
+            cudaEventRecord(a, r->stream);
+        }
+    }
+    cudaEvent_t take() {
+        if (!r->pool.empty()) {
+            cudaEvent_t e = r->pool.back();
+            r->pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void kernels(uint64_t n) {
+        r->launches[stage] += n;
+        r->total_launches += n;
+    }
+    ~StageScope() {
+        if (r->prof_on && a) {
+            cudaEvent_t b = take();
+            cudaEventRecord(b, r->stream);
+            r->pending.push_back({stage, a, b});
+        }
+    }
 };
 
 // ------------------------------------------------------------------------------ helpers
@@ -195,6 +238,8 @@ static uint32_t pick_batch(gpsb_renderer* r, uint32_t count) {
 
 static gpsb_status geometry(gpsb_renderer* r, const FrameConst& f) {
     if (r->n == 0) return GPSB_OK;
+    StageScope sc(r, GPSB_STAGE_GEOMETRY);
+    sc.kernels(1);
     launch_geometry(f, r->splats.as<float4>(), r->sh.as<float>(), r->lut.as<float>(), r->rec.as<float4>(),
                     r->cdesc.as<uint2>(), r->colour.as<float4>(), r->stream);
     CK(r, cudaGetLastError(), "geometry kernel");
@@ -206,23 +251,42 @@ static gpsb_status render_batch(gpsb_renderer* r, const FrameConst& f, bool part
                                 float4* accum) {
     uint64_t PS = sub_per_ensemble(r);
     ull_t* stats = r->stats.as<ull_t>();
-    CK(r, cudaMemsetAsync(r->sub.p, 0xFF, (size_t)E * PS * 8, r->stream), "clear subpixels");
-    launch_add_stat(stats, ST_ENSEMBLES, E, r->stream);
+    {
+        StageScope sc(r, GPSB_STAGE_CLEAR);
+        sc.kernels(1);
+        CK(r, cudaMemsetAsync(r->sub.p, 0xFF, (size_t)E * PS * 8, r->stream), "clear subpixels");
+        launch_add_stat(stats, ST_ENSEMBLES, E, r->stream);
+    }
     uint32_t* cnt = r->counters.as<uint32_t>();
     if (particles) {
-        launch_count_scan(f, r->cdesc.as<uint2>(), first_seed, E, r->lookback.as<uint64_t>(), cnt, r->clist.as<uint2>(),
-                          r->etot.as<EnsTotal>(), stats, r->err.as<uint32_t>(), r->stream);
-        CK(r, cudaGetLastError(), "count/scan kernel");
-        launch_particles(f, r->rec.as<float4>(), r->lut.as<float>(), r->clist.as<uint2>(), r->etot.as<EnsTotal>(),
-                         first_seed, E, r->sub.as<ull_t>(), cnt + 1, stats, r->sm_count * 4, r->stream);
-        CK(r, cudaGetLastError(), "particle kernel");
+        {
+            StageScope sc(r, GPSB_STAGE_COUNT_SCAN);
+            sc.kernels(1);
+            launch_count_scan(f, r->cdesc.as<uint2>(), first_seed, E, r->lookback.as<uint64_t>(), cnt,
+                              r->clist.as<uint2>(), r->etot.as<EnsTotal>(), stats, r->err.as<uint32_t>(), r->stream);
+            CK(r, cudaGetLastError(), "count/scan kernel");
+        }
+        {
+            StageScope sc(r, GPSB_STAGE_PARTICLES);
+            sc.kernels(1);
+            launch_particles(f, r->rec.as<float4>(), r->lut.as<float>(), r->clist.as<uint2>(), r->etot.as<EnsTotal>(),
+                             first_seed, E, r->sub.as<ull_t>(), cnt + 1, stats, r->sm_count * 4, r->stream);
+            CK(r, cudaGetLastError(), "particle kernel");
+        }
     } else {
+        StageScope sc(r, GPSB_STAGE_PRIMITIVE);
+        sc.kernels(1);
         launch_primitive(f, r->rec.as<float4>(), r->cdesc.as<uint2>(), r->lut.as<float>(), first_seed, E,
                          r->sub.as<ull_t>(), r->etot.as<EnsTotal>(), stats, r->stream);
         CK(r, cudaGetLastError(), "primitive kernel");
     }
-    launch_resolve(f, r->sub.as<ull_t>(), r->etot.as<EnsTotal>(), r->colour.as<float4>(), E, accum, stats, r->stream);
-    CK(r, cudaGetLastError(), "resolve kernel");
+    {
+        StageScope sc(r, GPSB_STAGE_RESOLVE);
+        sc.kernels(1);
+        launch_resolve(f, r->sub.as<ull_t>(), r->etot.as<EnsTotal>(), r->colour.as<float4>(), E, accum, stats,
+                       r->stream);
+        CK(r, cudaGetLastError(), "resolve kernel");
+    }
     r->last_batch = E;
     r->last_particle = particles;
     return GPSB_OK;
@@ -259,6 +323,8 @@ static void to_stats(const unsigned long long* w, gpsb_stats* out, uint32_t issu
     out->probe_demand = w[ST_PROBE];
     out->issue = issue;
     out->_pad = 0;
+    out->subpixel_writes = w[ST_WRITES];
+    out->list_entries = w[ST_ENTRIES];
 }
 
 static void poll_stats(gpsb_renderer* r) {
@@ -369,6 +435,11 @@ void gpsb_destroy(gpsb_renderer* r) {
                       &r->sub, &r->clist, &r->lookback, &r->etot, &r->counters, &r->rgba8};
     for (DevBuf* b : bufs) b->release();
     sorted_release(r->sorted);
+    for (auto& pe : r->pending) {
+        cudaEventDestroy(pe.a);
+        cudaEventDestroy(pe.b);
+    }
+    for (cudaEvent_t e : r->pool) cudaEventDestroy(e);
     if (r->stats_pinned) cudaFreeHost(r->stats_pinned);
     if (r->stats_event) cudaEventDestroy(r->stats_event);
     if (r->own) cudaStreamDestroy(r->own);
@@ -545,8 +616,13 @@ gpsb_status gpsb_render_sorted(gpsb_renderer* r, const gpsb_camera* cam, const g
     q.method = GPSB_METHOD_GPS;  // gps.rs:935
     FrameConst f = make_frame(r, *cam, q);
     std::string msg;
-    cudaError_t e = sorted_render(r->sorted, f, r->splats.as<float4>(), r->sh.as<float>(), r->accum.as<float4>(),
-                                  r->stats.as<unsigned long long>(), r->err.as<uint32_t>(), r->sm_count, true, r->stream, &msg);
+    cudaError_t e;
+    {
+        StageScope sc(r, GPSB_STAGE_SORTED);
+        sc.kernels(10);
+        e = sorted_render(r->sorted, f, r->splats.as<float4>(), r->sh.as<float>(), r->accum.as<float4>(),
+                          r->stats.as<unsigned long long>(), r->err.as<uint32_t>(), r->sm_count, true, r->stream, &msg);
+    }
     if (e != cudaSuccess) return cuda_fail(r, e, msg.c_str());
     r->have_sorted = true;
     r->accumulated = std::max(as_ensembles, 1u);
@@ -560,8 +636,13 @@ gpsb_status gpsb_probe_demand(gpsb_renderer* r, const gpsb_camera* cam, const gp
     if (!cam || !p) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null camera or params");
     FrameConst f = make_frame(r, *cam, *p);
     std::string msg;
-    cudaError_t e = sorted_render(r->sorted, f, r->splats.as<float4>(), r->sh.as<float>(), r->accum.as<float4>(),
-                                  r->stats.as<unsigned long long>(), r->err.as<uint32_t>(), r->sm_count, false, r->stream, &msg);
+    cudaError_t e;
+    {
+        StageScope sc(r, GPSB_STAGE_SORTED);
+        sc.kernels(1);
+        e = sorted_render(r->sorted, f, r->splats.as<float4>(), r->sh.as<float>(), r->accum.as<float4>(),
+                          r->stats.as<unsigned long long>(), r->err.as<uint32_t>(), r->sm_count, false, r->stream, &msg);
+    }
     if (e != cudaSuccess) return cuda_fail(r, e, msg.c_str());
     return GPSB_OK;
 }
@@ -641,8 +722,12 @@ gpsb_status gpsb_composite_rgba8(gpsb_renderer* r, const gpsb_params* p, uint32_
     cudaSetDevice(r->device);
     size_t bytes = (size_t)out_w * out_h * 4;
     CK(r, r->rgba8.ensure(bytes), "composite target");
-    launch_composite(r->accum.as<float4>(), r->W, r->H, p->exposure, p->srgb_output ? 1u : 0u, out_w, out_h,
-                     r->rgba8.as<uchar4>(), r->stream);
+    {
+        StageScope sc(r, GPSB_STAGE_COMPOSITE);
+        sc.kernels(1);
+        launch_composite(r->accum.as<float4>(), r->W, r->H, p->exposure, p->srgb_output ? 1u : 0u, out_w, out_h,
+                         r->rgba8.as<uchar4>(), r->stream);
+    }
     CK(r, cudaGetLastError(), "composite kernel");
     CK(r, cudaMemcpyAsync(out, r->rgba8.p, bytes, cudaMemcpyDeviceToHost, r->stream), "read composite");
     CK(r, cudaStreamSynchronize(r->stream), "synchronise");
@@ -686,6 +771,44 @@ gpsb_status gpsb_debug_read_subpixels(gpsb_renderer* r, uint32_t slot, uint64_t*
     CK(r, cudaMemcpyAsync(packed, r->sub.as<uint64_t>() + (size_t)slot * PS, PS * 8, cudaMemcpyDeviceToHost, r->stream),
        "read subpixels");
     CK(r, cudaStreamSynchronize(r->stream), "synchronise");
+    return GPSB_OK;
+}
+
+static gpsb_status resolve_profile(gpsb_renderer* r) {
+    if (r->pending.empty()) return GPSB_OK;
+    CK(r, cudaStreamSynchronize(r->stream), "synchronise");
+    for (auto& pe : r->pending) {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, pe.a, pe.b) == cudaSuccess) r->ms[pe.stage] += t;
+        r->pool.push_back(pe.a);
+        r->pool.push_back(pe.b);
+    }
+    r->pending.clear();
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_profile_enable(gpsb_renderer* r, int enable) {
+    if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
+    cudaSetDevice(r->device);
+    gpsb_status s = resolve_profile(r);
+    if (s != GPSB_OK) return s;
+    r->prof_on = enable != 0;
+    memset(r->launches, 0, sizeof r->launches);
+    memset(r->ms, 0, sizeof r->ms);
+    r->total_launches = 0;
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_profile_read(gpsb_renderer* r, gpsb_profile* out) {
+    if (!r || !out) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(r->device);
+    gpsb_status s = resolve_profile(r);
+    if (s != GPSB_OK) return s;
+    for (int k = 0; k < GPSB_STAGES; ++k) {
+        out->launches[k] = r->launches[k];
+        out->ms[k] = r->ms[k];
+    }
+    out->total_launches = r->total_launches;
     return GPSB_OK;
 }
 

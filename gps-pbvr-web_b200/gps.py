@@ -112,11 +112,14 @@ class GpuStats:  # gps.rs:231-252
     ensembles: int = 0
     probe_demand: int = 0
     issue: int = 0
+    subpixel_writes: int = 0
+    list_entries: int = 0
 
     @staticmethod
     def from_c(s: abi.StatsC) -> "GpuStats":
         return GpuStats(s.points, s.truncated_splats, s.dropped_points, s.visible_splats, s.orphan_subpixels,
-                        s.candidates, s.undercovered_splats, s.skipped_ensembles, s.ensembles, s.probe_demand, s.issue)
+                        s.candidates, s.undercovered_splats, s.skipped_ensembles, s.ensembles, s.probe_demand, s.issue,
+                        s.subpixel_writes, s.list_entries)
 
     def counters(self):
         """Every counter but the readback issue number (for equality checks between paths)."""
@@ -405,6 +408,19 @@ class GpsRenderer:
 
     def debug_error_word(self) -> int:
         return self._L.gpsb_debug_error_word(self._r)
+
+    # ---------------------------------------------------------------- profiling
+    def profile_enable(self, on: bool = True):
+        self._ck(self._L.gpsb_profile_enable(self._r, int(on)))
+
+    def profile(self) -> dict:
+        p = abi.ProfileC()
+        self._ck(self._L.gpsb_profile_read(self._r, C.byref(p)))
+        return {"launches": {n: int(p.launches[i]) for i, n in enumerate(abi.STAGES)},
+                "ms": {n: float(p.ms[i]) for i, n in enumerate(abi.STAGES)}, "total_launches": int(p.total_launches)}
+
+    def set_stream(self, cuda_stream_ptr: int):
+        self._ck(self._L.gpsb_set_stream(self._r, C.c_void_p(cuda_stream_ptr) if cuda_stream_ptr else None))
 
 
 def default_params(**kw) -> RenderParams:

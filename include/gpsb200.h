@@ -108,7 +108,31 @@ typedef struct gpsb_stats {
     uint64_t probe_demand;
     uint32_t issue;
     uint32_t _pad;
+    /* no reference counterpart: particles written to an on-screen subpixel (the oracle's
+     * RenderStats::subpixel_writes, crates/gps-core/src/oracle.rs:99-104) and entries of the
+     * per-ensemble compact particle lists; they size the algorithmic bytes of the kernels */
+    uint64_t subpixel_writes;
+    uint64_t list_entries;
 } gpsb_stats;
+
+/* Device-time profile of the renderer's kernels (no reference counterpart; the reference has
+ * no GPU timestamps, gps.rs:888). Stages: */
+enum {
+    GPSB_STAGE_GEOMETRY = 0,
+    GPSB_STAGE_COUNT_SCAN = 1,
+    GPSB_STAGE_PARTICLES = 2,
+    GPSB_STAGE_RESOLVE = 3,
+    GPSB_STAGE_CLEAR = 4,
+    GPSB_STAGE_PRIMITIVE = 5,
+    GPSB_STAGE_SORTED = 6,
+    GPSB_STAGE_COMPOSITE = 7,
+    GPSB_STAGES = 8
+};
+typedef struct gpsb_profile {
+    uint64_t launches[8];    /* kernels of this library launched per stage */
+    double ms[8];            /* summed device time per stage (CUDA events on the renderer's stream) */
+    uint64_t total_launches; /* kernels launched since gpsb_create or the last gpsb_profile_enable */
+} gpsb_profile;
 
 typedef struct gpsb_renderer gpsb_renderer;
 
@@ -222,6 +246,12 @@ gpsb_status gpsb_debug_read_counts(gpsb_renderer* r, uint32_t slot, uint32_t* co
 gpsb_status gpsb_debug_read_subpixels(gpsb_renderer* r, uint32_t slot, uint64_t* packed);
 /* Device-side error word (bounded waits that gave up); 0 when healthy. */
 uint32_t gpsb_debug_error_word(gpsb_renderer* r);
+
+/* Stage timing: enable (1) or disable (0) CUDA-event timing of every stage; both reset the
+ * profile. Launch counting is always on. */
+gpsb_status gpsb_profile_enable(gpsb_renderer* r, int enable);
+/* Reads the profile (synchronises the renderer's stream). */
+gpsb_status gpsb_profile_read(gpsb_renderer* r, gpsb_profile* out);
 
 /* ------------------------------------------------------------------- PLY (gps-io) */
 /* load_ply (crates/gps-io/src/lib.rs:260-338) + activation (lib.rs:84-96) +

@@ -152,13 +152,14 @@ def render_monte_carlo(scene, cam17, w, h, spp_side, sets, bg, seed, footprint_s
 def render_particles_3d(scene, cam17, w, h, spp_side, sets, bg, seed, level=3, rule=1, radial_correction=False,
                         base_k=512.0, reference_pixel_length=0.01, near_z=0.05, low_pass_jitter=True,
                         centre_depth=False, linearized_projection=False, density_scale=1.0, per_particle_seed=False,
-                        threads=1):
+                        threads=1, max_points_per_splat=0xFFFFFFFF):
     """rule: 0 Proportional, 1 Extinction, 2 Dilog (crates/gps-core/src/lib.rs:296-300)."""
     s, n = _scene14(scene)
     img = np.zeros((h * w, 3))
     st = np.zeros(3)
     opt = _f64([level, rule, float(radial_correction), base_k, reference_pixel_length, near_z, float(low_pass_jitter),
-                float(centre_depth), float(linearized_projection), density_scale, float(per_particle_seed)])
+                float(centre_depth), float(linearized_projection), density_scale, float(per_particle_seed),
+                float(max_points_per_splat)])
     lib().o1_render_particles_3d(_p(s), n, _p(_f64(cam17, 17)), w, h, spp_side, sets, _p(_f64(bg, 3)), seed, _p(opt),
                                  _p(img), _p(st), threads)
     return img, {"points": st[0], "candidates": st[1], "subpixel_writes": st[2]}
@@ -197,14 +198,14 @@ def _o2_scene(splats, sh):
 
 def o2_render_ensembles(splats, sh, sh_degree, lut, w, h, spp_side, cam17, params, first_seed, count, accum=None,
                         stats=None, want_counts=False, want_packed=False):
-    """Returns (accum (h*w,4) f32, stats (10,) u64, counts (count,n) u32 | None, packed (count,h*w*S) u64 | None)."""
+    """Returns (accum (h*w,4) f32, stats (12,) u64, counts (count,n) u32 | None, packed (count,h*w*S) u64 | None)."""
     import ctypes
     g, s = _o2_scene(splats, sh)
     n = g.shape[0]
     side = max(1, min(int(spp_side), 4))
     S = side * side
     acc = np.zeros((h * w, 4), np.float32) if accum is None else np.ascontiguousarray(accum, np.float32).copy()
-    st = np.zeros(10, np.uint64) if stats is None else np.ascontiguousarray(stats, np.uint64).copy()
+    st = np.zeros(12, np.uint64) if stats is None else np.ascontiguousarray(stats, np.uint64).copy()
     counts = np.zeros((count, n), np.uint32) if want_counts else None
     packed = np.zeros((count, h * w * S), np.uint64) if want_packed else None
     lut = np.ascontiguousarray(lut, np.float32)
@@ -219,7 +220,7 @@ def o2_render_sorted(splats, sh, sh_degree, lut, w, h, spp_side, cam17, params):
     g, s = _o2_scene(splats, sh)
     n = g.shape[0]
     acc = np.zeros((h * w, 4), np.float32)
-    st = np.zeros(10, np.uint64)
+    st = np.zeros(12, np.uint64)
     keys = np.zeros(n, np.uint32)
     vals = np.zeros(n, np.uint32)
     lib().o2_render_sorted(_p(g), n, _p(s), sh_degree, _p(np.ascontiguousarray(lut, np.float32)), w, h, spp_side,

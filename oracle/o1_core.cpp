@@ -542,6 +542,9 @@ struct POptions {  // oracle.rs:317-350
     int low_pass_jitter, centre_depth, linearized_projection;
     double density_scale;
     int per_particle_seed;
+    // Per-splat cap on the candidate count as the GPU applies it (gps_splat.wgsl:597-602);
+    // 0xFFFFFFFF = none (the oracle's own behaviour).
+    uint32_t max_points_per_splat;
 };
 static M3 cholesky_3d(const M3& c) {  // oracle.rs:352-361
     double a00 = c.c[0].x, a10 = c.c[0].y, a20 = c.c[0].z, a11 = c.c[1].y, a21 = c.c[1].z, a22 = c.c[2].z;
@@ -571,6 +574,7 @@ static void particle_sets(const std::vector<Prep>& preps, const Camera& cam, con
                                                    : RandStream(particle_seed(true, (uint32_t)gid, 1, set_seed));
             int32_t n = poisson_sample(p.lambda, rng);
             st.candidates += (double)n;
+            if ((uint32_t)n > opt.max_points_per_splat) n = (int32_t)opt.max_points_per_splat;
             for (int32_t k = 0; k < n; ++k) {
                 if (opt.per_particle_seed) rng = RandStream(particle_seed(true, p.index, (uint32_t)k + 1u, set_seed));
                 // MSVC right-to-left argument order: z, y, x (oracle.rs:445-451)
@@ -808,12 +812,13 @@ void o1_render_monte_carlo(const double* scene, size_t n, const double* cam, siz
     render_monte_carlo(s.data(), n, unpack_cam(cam), w, h, side, sets, {bg[0], bg[1], bg[2]}, seed, o, (V3*)img, st, threads);
     stats3[0] = st.points; stats3[1] = st.candidates; stats3[2] = st.subpixel_writes;
 }
-// opt: level, rule, radial, base_k, refl, near, jitter, centre, linearized, density, per_particle_seed
+// opt: level, rule, radial, base_k, refl, near, jitter, centre, linearized, density, per_particle_seed, cap
 void o1_render_particles_3d(const double* scene, size_t n, const double* cam, size_t w, size_t h, size_t side, size_t sets,
-                            const double* bg, uint32_t seed, const double* opt11, double* img, double* stats3, int threads) {
+                            const double* bg, uint32_t seed, const double* opt12, double* img, double* stats3, int threads) {
     auto s = unpack(scene, n);
-    POptions o = {(int)opt11[0], (int)opt11[1], (int)opt11[2], opt11[3], opt11[4], opt11[5],
-                  (int)opt11[6], (int)opt11[7], (int)opt11[8], opt11[9], (int)opt11[10]};
+    POptions o = {(int)opt12[0], (int)opt12[1], (int)opt12[2], opt12[3], opt12[4], opt12[5],
+                  (int)opt12[6], (int)opt12[7], (int)opt12[8], opt12[9], (int)opt12[10],
+                  opt12[11] >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)opt12[11]};
     RenderStats st;
     render_particles_3d(s.data(), n, unpack_cam(cam), w, h, side, sets, {bg[0], bg[1], bg[2]}, seed, o, (V3*)img, st, threads);
     stats3[0] = st.points; stats3[1] = st.candidates; stats3[2] = st.subpixel_writes;

@@ -600,8 +600,9 @@ int o2_render_ensembles(const gpsb_gaussian* g, uint32_t n, const float* sh, uin
     Scene s = make_scene(g, n, sh, sh_degree, lut);
     Stats st;
     memset(&st, 0, sizeof st);
-    // stats layout in: points, truncated, dropped, visible, orphan, candidates, undercovered, skipped, ensembles, probe
-    for (int k = 0; k < 10; ++k) st.c[k] = stats[k];
+    // stats layout: points, truncated, dropped, visible, orphan, candidates, undercovered, skipped, ensembles,
+    // probe, subpixel writes, compact-list entries
+    for (int k = 0; k < 12; ++k) st.c[k] = stats[k];
     const uint32_t S = side * side;
     const size_t nsub = (size_t)W * H * S;
     std::vector<uint32_t> depth(nsub), winner(nsub);
@@ -621,6 +622,7 @@ int o2_render_ensembles(const gpsb_gaussian* g, uint32_t n, const float* sh, uin
             pl.offsets.assign(n, 0u);
             for (uint32_t i = 0; i < n; ++i) pl.offsets[i] = pl.prepare(i);
             if (counts_out) memcpy(counts_out + (size_t)e * n, pl.offsets.data(), (size_t)n * 4);
+            for (uint32_t i = 0; i < n; ++i) st.c[11] += pl.offsets[i] ? 1u : 0u;
             // finalize_dispatch (gps_splat.wgsl:648-663): skip the ensemble on u32 overflow
             if (pl.overflow) {
                 st.c[7] += 1;
@@ -632,6 +634,7 @@ int o2_render_ensembles(const gpsb_gaussian* g, uint32_t n, const float* sh, uin
             if (counts_out) memset(counts_out + (size_t)e * n, 0, (size_t)n * 4);
             for (uint32_t i = 0; i < n; ++i) pl.splat_pass(i);
         }
+        st.c[10] += pl.writes.size();
         // depth pass, then colour pass among the depth winners (gps_splat.wgsl:276-281)
         for (const Write& w : pl.writes) depth[w.idx] = std::min(depth[w.idx], w.key);
         for (const Write& w : pl.writes)
@@ -664,7 +667,7 @@ int o2_render_ensembles(const gpsb_gaussian* g, uint32_t n, const float* sh, uin
             }
         }
     }
-    for (int k = 0; k < 10; ++k) stats[k] = st.c[k];
+    for (int k = 0; k < 12; ++k) stats[k] = st.c[k];
     return 0;
 }
 

@@ -41,7 +41,8 @@ def o2_render(splats, sh, degree, W, H, side, cam, params, first_seed, count):
 
 def stats_tuple(st):
     return (st.points, st.truncated_splats, st.dropped_points, st.visible_splats, st.orphan_subpixels, st.candidates,
-            st.undercovered_splats, st.skipped_ensembles, st.ensembles, st.probe_demand)
+            st.undercovered_splats, st.skipped_ensembles, st.ensembles, st.probe_demand, st.subpixel_writes,
+            st.list_entries)
 
 
 def assert_bit_exact(splats, sh, degree, W, H, side, cam, params, first_seed=1, count=3):
