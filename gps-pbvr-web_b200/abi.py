@@ -101,6 +101,7 @@ SIGNATURES = {
     "gpsb_ply_last_error": (C.c_char_p, []),
     "gpsb_profile_enable": (ST, [P, C.c_int]),
     "gpsb_profile_read": (ST, [P, P]),
+    "gpsb_sort_pairs_noalloc": (ST, [P, P, P, P, U32, U32, P, P]),
 }
 
 _lib = None

@@ -23,6 +23,10 @@ void host_radius_lut(float* out);  // hostmath.cpp
 
 static thread_local std::string g_last_error;
 
+namespace gpsb {
+void set_global_error(const char* msg) { g_last_error = msg; }
+}
+
 static const size_t kMaxSplats = 16000000;  // gps.rs:24
 static const uint32_t kDefaultBatch = 64;
 

@@ -14,9 +14,12 @@
 //   k_composite     gps_composite.wgsl:41-55 into a headless RGBA8 buffer.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 
 #include <algorithm>
+#include <mutex>
 
+#include "../../include/gpsb200.h"
 #include "devmath.cuh"
 #include "sorted.h"
 
@@ -214,11 +217,49 @@ static cudaError_t radix_impl(RadixScratch& s, uint32_t* ka, uint32_t* va, uint3
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------- no-allocation sort
+// Callers that may not allocate device memory (a host application that owns the whole GPU memory
+// budget through its own pool, or a real-time frame loop where a cudaMalloc would stall or is
+// forbidden) use gpsb_sort_pairs_noalloc. Its scratch (digit histograms, tile counters and the
+// lookback words) is this file-scope array, sized for kNoAllocMaxN pairs with up to 32-bit keys
+// (4 passes of 8-bit digits): about 2.2 MB that every GPU which loads the library keeps until the
+// process exits.
+constexpr uint32_t kNoAllocMaxN = 1u << 21;
+constexpr uint32_t kNoAllocTiles = (kNoAllocMaxN + kRsTile - 1) / kRsTile;
+constexpr uint32_t kNoAllocPasses = 4;
+constexpr size_t kNoAllocHistWords = kNoAllocPasses * 256;
+constexpr size_t kNoAllocCounterWords = 16;  // per-pass tile counters, then the default error word
+constexpr size_t kNoAllocWords = kNoAllocHistWords + kNoAllocCounterWords + (size_t)kNoAllocPasses * kNoAllocTiles * 256;
+static __device__ __align__(256) uint32_t g_noalloc_sort_scratch[kNoAllocWords];
+
 cudaError_t radix_sort_pairs(RadixScratch& s, uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, uint32_t n,
                              int key_bits, int digit_bits, uint32_t* err, cudaStream_t st) {
     if (digit_bits == 4) return radix_impl<4>(s, ka, va, kb, vb, n, key_bits, err, st);
     if (digit_bits == 6) return radix_impl<6>(s, ka, va, kb, vb, n, key_bits, err, st);
     return radix_impl<8>(s, ka, va, kb, vb, n, key_bits, err, st);
+}
+
+// Device address of g_noalloc_sort_scratch on the current device, resolved once per device. In host
+// code the array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress with the device current; it is cached per device ordinal.
+static void* noalloc_scratch_address(cudaError_t* err) {
+    static std::mutex mu;
+    static void* addr[256] = {};
+    int dev = 0;
+    *err = cudaGetDevice(&dev);
+    if (*err != cudaSuccess) return nullptr;
+    if (dev < 0 || dev >= 256) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        *err = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+        if (*err != cudaSuccess) return nullptr;
+        addr[dev] = p;
+    }
+    return addr[dev];
 }
 
 // ============================================================================ u32 exclusive scan
@@ -630,3 +671,74 @@ void launch_composite(const float4* accum, uint32_t W, uint32_t H, float exposur
 }
 
 }  // namespace gpsb
+
+// ============================================================================ C ABI: no-allocation sort
+namespace gpsb {
+void set_global_error(const char* msg);  // renderer.cpp: message of gpsb_last_error(NULL)
+}
+static thread_local char g_noalloc_error[256];
+
+extern "C" gpsb_status gpsb_sort_pairs_noalloc(uint32_t* keys_in, uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                                               uint32_t n, uint32_t key_bits, void* cuda_stream, uint32_t* err_dev) {
+    using namespace gpsb;
+    g_noalloc_error[0] = 0;
+    if (n > kNoAllocMaxN) {
+        snprintf(g_noalloc_error, sizeof g_noalloc_error,
+                 "gpsb_sort_pairs_noalloc: %u pairs exceed the fixed scratch of %u pairs", n, kNoAllocMaxN);
+        set_global_error(g_noalloc_error);
+        return GPSB_ERR_LIMIT;
+    }
+    if (key_bits < 1 || key_bits > 32) {
+        snprintf(g_noalloc_error, sizeof g_noalloc_error, "gpsb_sort_pairs_noalloc: key_bits must be 1..32");
+        set_global_error(g_noalloc_error);
+        return GPSB_ERR_INVALID_ARGUMENT;
+    }
+    if (n == 0) return GPSB_OK;
+    if (!keys_in || !vals_in || !keys_out || !vals_out) {
+        snprintf(g_noalloc_error, sizeof g_noalloc_error, "gpsb_sort_pairs_noalloc: null buffer");
+        set_global_error(g_noalloc_error);
+        return GPSB_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    cudaError_t e;
+    uint32_t* base = (uint32_t*)noalloc_scratch_address(&e);
+    if (!base) {
+        snprintf(g_noalloc_error, sizeof g_noalloc_error, "gpsb_sort_pairs_noalloc: scratch address: %s",
+                 cudaGetErrorString(e));
+        set_global_error(g_noalloc_error);
+        return GPSB_ERR_CUDA;
+    }
+    const int passes = (int)((key_bits + 7) / 8);
+    const uint32_t tiles = (n + kRsTile - 1) / kRsTile;
+    uint32_t* hist = base;
+    uint32_t* counters = base + kNoAllocHistWords;
+    uint32_t* err = err_dev ? err_dev : counters + kNoAllocPasses;
+    uint32_t* lookback = base + kNoAllocHistWords + kNoAllocCounterWords;
+    // the array keeps the previous call's contents: clear what this call needs at zero
+    e = cudaMemsetAsync(base, 0, (kNoAllocHistWords + kNoAllocCounterWords) * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(lookback, 0, (size_t)passes * tiles * 256 * 4, st);
+    uint32_t *ik = keys_in, *iv = vals_in, *ok = keys_out, *ov = vals_out;
+    if (e == cudaSuccess && passes % 2 == 0) {
+        // an even number of passes ends in the first buffer: start from a copy in the output
+        e = cudaMemcpyAsync(keys_out, keys_in, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(vals_out, vals_in, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+        ik = keys_out; iv = vals_out; ok = keys_in; ov = vals_in;
+    }
+    if (e == cudaSuccess) {
+        k_radix_hist<8><<<std::min<uint32_t>((n + 4095) / 4096, 1184u), 256, 0, st>>>(ik, n, passes, hist);
+        k_radix_hist_scan<8><<<1, 32, 0, st>>>(hist, passes);
+        for (int p = 0; p < passes; ++p) {
+            k_onesweep<8><<<tiles, kRsThreads, 0, st>>>(ik, iv, ok, ov, n, p * 8, hist + p * 256,
+                                                        lookback + (size_t)p * tiles * 256, counters + p, err);
+            std::swap(ik, ok);
+            std::swap(iv, ov);
+        }
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        snprintf(g_noalloc_error, sizeof g_noalloc_error, "gpsb_sort_pairs_noalloc: %s", cudaGetErrorString(e));
+        set_global_error(g_noalloc_error);
+        return GPSB_ERR_CUDA;
+    }
+    return GPSB_OK;
+}

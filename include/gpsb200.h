@@ -253,6 +253,27 @@ gpsb_status gpsb_profile_enable(gpsb_renderer* r, int enable);
 /* Reads the profile (synchronises the renderer's stream). */
 gpsb_status gpsb_profile_read(gpsb_renderer* r, gpsb_profile* out);
 
+/* ------------------------------------------------------------------- sort without allocation */
+/* No counterpart in the reference. Stable ascending LSD radix sort of n (key, value) pairs on
+ * the low key_bits bits (1..32, keys must be below 2^key_bits), the onesweep kernels of the
+ * depth-sorted path, for callers that cannot allocate device memory: a host that owns the whole
+ * GPU memory budget through its own pool, or a real-time frame loop in which a cudaMalloc would
+ * stall or is not allowed. It allocates nothing: all four pointers are device memory of the
+ * caller; the sorted pairs are written to keys_out/vals_out and keys_in/vals_in are overwritten
+ * (they are the ping-pong buffer). Its scratch is a fixed array inside this library (about
+ * 2.2 MB, held by every GPU that loads the library until the process exits), which limits n to
+ * 2,097,152 pairs; larger n returns GPSB_ERR_LIMIT. The first call on a device looks the array's
+ * device address up (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture. Work is enqueued on cuda_stream (NULL = the legacy default stream)
+ * and the call returns without waiting. Every call shares the one array, which keeps the last
+ * call's contents: each call clears what it needs, but calls that overlap on the GPU (on
+ * different streams, or from several threads) race and give wrong results. A bounded device-side
+ * wait that gives up ORs a non-zero value into *err_dev (a device word of the caller; NULL uses a
+ * word inside the array). Messages of failed calls: gpsb_last_error(NULL). */
+gpsb_status gpsb_sort_pairs_noalloc(uint32_t* keys_in, uint32_t* vals_in, uint32_t* keys_out,
+                                    uint32_t* vals_out, uint32_t n, uint32_t key_bits,
+                                    void* cuda_stream, uint32_t* err_dev);
+
 /* ------------------------------------------------------------------- PLY (gps-io) */
 /* load_ply (crates/gps-io/src/lib.rs:260-338) + activation (lib.rs:84-96) +
  * GpuGaussian::from_activated (gps.rs:41-49), parsed on the host. Two calls: first with
