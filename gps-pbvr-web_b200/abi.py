@@ -48,6 +48,11 @@ class ProfileC(C.Structure):
     _fields_ = [("launches", C.c_uint64 * 8), ("ms", C.c_double * 8), ("total_launches", C.c_uint64)]
 
 
+class TuningC(C.Structure):
+    _fields_ = [("sort_digit_bits", C.c_uint32), ("blend_tile_w", C.c_uint32), ("blend_tile_h", C.c_uint32),
+                ("particle_items", C.c_uint32), ("particle_blocks_per_sm", C.c_uint32), ("ensemble_batch", C.c_uint32)]
+
+
 STAGES = ["geometry", "count_scan", "particles", "resolve", "clear", "primitive", "sorted", "composite"]
 
 
@@ -102,6 +107,8 @@ SIGNATURES = {
     "gpsb_profile_enable": (ST, [P, C.c_int]),
     "gpsb_profile_read": (ST, [P, P]),
     "gpsb_sort_pairs_noalloc": (ST, [P, P, P, P, U32, U32, P, P]),
+    "gpsb_set_tuning": (ST, [P, P]),
+    "gpsb_get_tuning": (ST, [P, P]),
 }
 
 _lib = None

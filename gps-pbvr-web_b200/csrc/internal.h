@@ -80,7 +80,7 @@ void launch_count_scan(const FrameConst& fc, const uint2* cdesc, uint32_t first_
                        uint32_t* err, cudaStream_t st);
 void launch_particles(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
                       const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
-                      uint32_t* unit_counter, unsigned long long* stats, int grid, cudaStream_t st);
+                      uint32_t* unit_counter, unsigned long long* stats, int grid, int items, cudaStream_t st);
 void launch_primitive(const FrameConst& fc, const float4* rec, const uint2* cdesc, const float* lut,
                       uint32_t first_seed, uint32_t E, unsigned long long* sub, EnsTotal* etot,
                       unsigned long long* stats, cudaStream_t st);

@@ -456,8 +456,6 @@ __device__ __forceinline__ uint32_t emit_so(const FrameConst& f, uint32_t i, uin
 }
 
 constexpr int kPT = 256;               // threads per particle block
-constexpr int kPIPT = 8;               // particles per thread per tile
-constexpr int kPTile = kPT * kPIPT;    // particles per tile
 constexpr int kMaxE = 1024;            // ensembles per batch (shared prefix table)
 
 // Largest j in [lo, hi) with off(j) <= v, by a 32-ary warp search (off(lo) <= v must hold).
@@ -481,15 +479,18 @@ __device__ __forceinline__ uint32_t warp_last_le(const uint2* __restrict__ L, ui
 // the compact list, regenerates it from its own stream particle_seed(i, k + 1, seed) and writes it
 // with one 64-bit atomicMin of (depth key << 32 | i), which equals the reference's depth pass
 // followed by the colour pass (gps_splat.wgsl:276-281). Ensembles flagged skipped get no work.
-template <int MC>  // 0 GPS, 1 PBVR, 2 ScreenOccupancy
+template <int MC, int kPIPT>  // MC: 0 GPS, 1 PBVR, 2 ScreenOccupancy; kPIPT: particles per thread per tile
 __global__ void __launch_bounds__(kPT) k_particles(FrameConst f, const float4* __restrict__ rec,
                                                    const float* __restrict__ lut, const uint2* __restrict__ clist,
                                                    const EnsTotal* __restrict__ etot, uint32_t first_seed, uint32_t E,
                                                    ull* sub, uint32_t* unit_counter, ull* stats) {
-    extern __shared__ float s_lut[];  // kLutN floats when GPS with the table radius
+    constexpr int kPTile = kPT * kPIPT;  // particles per tile
+    // dynamic shared memory: [entry offsets (kPTile + 2)] [entry ids (kPTile + 2)] [radius table (GPS)]
+    extern __shared__ uint32_t s_dyn[];
+    uint32_t* s_off = s_dyn;
+    uint32_t* s_id = s_dyn + (kPTile + 2);
+    float* s_lut = reinterpret_cast<float*>(s_dyn + 2 * (kPTile + 2));
     __shared__ uint64_t s_ubase[kMaxE + 1];
-    __shared__ uint32_t s_off[kPTile + 2];
-    __shared__ uint32_t s_id[kPTile + 2];
     __shared__ uint32_t s_unit, s_j0, s_w;
     const int tid = threadIdx.x, lane = tid & 31;
     const bool use_lut = MC == 0 && !f.exact_radius;
@@ -600,24 +601,43 @@ __global__ void __launch_bounds__(kPT) k_particles(FrameConst f, const float4* _
     if (lane == 0 && wv) atomicAdd(&stats[ST_WRITES], wv);
 }
 
+template <int MC, int IPT>
+static void launch_particles_t(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
+                               const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
+                               uint32_t* unit_counter, unsigned long long* stats, int grid, cudaStream_t st) {
+    size_t smem = 2 * (kPT * IPT + 2) * sizeof(uint32_t);
+    if (MC == 0 && !fc.exact_radius) smem += kLutN * sizeof(float);
+    static size_t attr = 0;
+    if (smem > 48 * 1024 && smem > attr) {
+        cudaFuncSetAttribute(k_particles<MC, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = smem;
+    }
+    k_particles<MC, IPT><<<grid, kPT, smem, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
+}
+
+template <int IPT>
+static void launch_particles_m(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
+                               const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
+                               uint32_t* unit_counter, unsigned long long* stats, int grid, cudaStream_t st) {
+    if (fc.method == 0u)
+        launch_particles_t<0, IPT>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+    else if (fc.method == 4u)
+        launch_particles_t<2, IPT>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+    else
+        launch_particles_t<1, IPT>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+}
+
 void launch_particles(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
                       const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
-                      uint32_t* unit_counter, unsigned long long* stats, int grid, cudaStream_t st) {
+                      uint32_t* unit_counter, unsigned long long* stats, int grid, int items, cudaStream_t st) {
     cudaMemsetAsync(unit_counter, 0, sizeof(uint32_t), st);
     if (fc.N == 0 || E == 0) return;
-    if (fc.method == 0u) {
-        size_t smem = fc.exact_radius ? 0 : kLutN * sizeof(float);
-        static bool attr_set = false;
-        if (!attr_set) {
-            cudaFuncSetAttribute(k_particles<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kLutN * sizeof(float)));
-            attr_set = true;
-        }
-        k_particles<0><<<grid, kPT, smem, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
-    } else if (fc.method == 4u) {
-        k_particles<2><<<grid, kPT, 0, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
-    } else {
-        k_particles<1><<<grid, kPT, 0, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
-    }
+    if (items >= 24)
+        launch_particles_m<24>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+    else if (items >= 16)
+        launch_particles_m<16>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+    else
+        launch_particles_m<8>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
 }
 
 // ============================================================================ primitive path

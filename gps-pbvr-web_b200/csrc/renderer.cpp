@@ -28,7 +28,6 @@ void set_global_error(const char* msg) { g_last_error = msg; }
 }
 
 static const size_t kMaxSplats = 16000000;  // gps.rs:24
-static const uint32_t kDefaultBatch = 64;
 
 struct DevBuf {
     void* p = nullptr;
@@ -93,6 +92,8 @@ struct gpsb_renderer {
     uint64_t launches[GPSB_STAGES] = {};
     double ms[GPSB_STAGES] = {};
     uint64_t total_launches = 0;
+    // launch-shape tuning
+    uint32_t particle_items = 8, particle_blocks_per_sm = 4, ensemble_batch = 64;
 };
 
 // Brackets the kernels of one stage with CUDA events on the renderer's stream (when profiling)
@@ -229,7 +230,7 @@ static gpsb_status ensure_batch(gpsb_renderer* r, uint32_t E) {
 // Ensembles per batch: up to kDefaultBatch, fewer when the per-ensemble buffers would exceed
 // a quarter of the free device memory.
 static uint32_t pick_batch(gpsb_renderer* r, uint32_t count) {
-    uint32_t want = std::min(count, kDefaultBatch);
+    uint32_t want = std::min(count, r->ensemble_batch);
     if (want <= r->batch_cap) return want;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
@@ -274,7 +275,8 @@ static gpsb_status render_batch(gpsb_renderer* r, const FrameConst& f, bool part
             StageScope sc(r, GPSB_STAGE_PARTICLES);
             sc.kernels(1);
             launch_particles(f, r->rec.as<float4>(), r->lut.as<float>(), r->clist.as<uint2>(), r->etot.as<EnsTotal>(),
-                             first_seed, E, r->sub.as<ull_t>(), cnt + 1, stats, r->sm_count * 4, r->stream);
+                             first_seed, E, r->sub.as<ull_t>(), cnt + 1, stats,
+                             r->sm_count * (int)r->particle_blocks_per_sm, (int)r->particle_items, r->stream);
             CK(r, cudaGetLastError(), "particle kernel");
         }
     } else {
@@ -775,6 +777,51 @@ gpsb_status gpsb_debug_read_subpixels(gpsb_renderer* r, uint32_t slot, uint64_t*
     CK(r, cudaMemcpyAsync(packed, r->sub.as<uint64_t>() + (size_t)slot * PS, PS * 8, cudaMemcpyDeviceToHost, r->stream),
        "read subpixels");
     CK(r, cudaStreamSynchronize(r->stream), "synchronise");
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_set_tuning(gpsb_renderer* r, const gpsb_tuning* t) {
+    if (!r || !t) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null argument");
+    if (t->sort_digit_bits && t->sort_digit_bits != 4 && t->sort_digit_bits != 6 && t->sort_digit_bits != 8)
+        return fail(r, GPSB_ERR_INVALID_ARGUMENT, "sort_digit_bits must be 4, 6 or 8");
+    if (t->blend_tile_w || t->blend_tile_h) {
+        bool ok = (t->blend_tile_w == 16 && t->blend_tile_h == 16) || (t->blend_tile_w == 32 && t->blend_tile_h == 8) ||
+                  (t->blend_tile_w == 32 && t->blend_tile_h == 32);
+        if (!ok) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "blend tiles must be 16x16, 32x8 or 32x32");
+    }
+    if (t->particle_items && t->particle_items != 8 && t->particle_items != 16 && t->particle_items != 24)
+        return fail(r, GPSB_ERR_INVALID_ARGUMENT, "particle_items must be 8, 16 or 24");
+    if (t->particle_blocks_per_sm > 32) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "particle_blocks_per_sm must be 1..32");
+    if (t->ensemble_batch > 1024) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "ensemble_batch must be 1..1024");
+    cudaSetDevice(r->device);
+    CK(r, cudaStreamSynchronize(r->stream), "synchronise");
+    if (t->sort_digit_bits) r->sorted.digit_bits = (int)t->sort_digit_bits;
+    if (t->blend_tile_w) {
+        if (r->sorted.tw != t->blend_tile_w || r->sorted.th != t->blend_tile_h) r->have_sorted = false;
+        r->sorted.tw = t->blend_tile_w;
+        r->sorted.th = t->blend_tile_h;
+    }
+    if (t->particle_items) r->particle_items = t->particle_items;
+    if (t->particle_blocks_per_sm) r->particle_blocks_per_sm = t->particle_blocks_per_sm;
+    if (t->ensemble_batch) {
+        r->ensemble_batch = t->ensemble_batch;
+        r->batch_cap = 0;
+        r->sub.release();
+        r->clist.release();
+        r->lookback.release();
+        r->etot.release();
+    }
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_get_tuning(const gpsb_renderer* r, gpsb_tuning* out) {
+    if (!r || !out) return GPSB_ERR_INVALID_ARGUMENT;
+    out->sort_digit_bits = (uint32_t)r->sorted.digit_bits;
+    out->blend_tile_w = r->sorted.tw;
+    out->blend_tile_h = r->sorted.th;
+    out->particle_items = r->particle_items;
+    out->particle_blocks_per_sm = r->particle_blocks_per_sm;
+    out->ensemble_batch = r->ensemble_batch;
     return GPSB_OK;
 }
 

@@ -419,6 +419,21 @@ class GpsRenderer:
         return {"launches": {n: int(p.launches[i]) for i, n in enumerate(abi.STAGES)},
                 "ms": {n: float(p.ms[i]) for i, n in enumerate(abi.STAGES)}, "total_launches": int(p.total_launches)}
 
+    def set_tuning(self, **kw):
+        """sort_digit_bits, blend_tile_w, blend_tile_h, particle_items, particle_blocks_per_sm, ensemble_batch."""
+        t = abi.TuningC()
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self._ck(self._L.gpsb_set_tuning(self._r, C.byref(t)))
+
+    def tuning(self) -> dict:
+        t = abi.TuningC()
+        self._ck(self._L.gpsb_get_tuning(self._r, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def set_sort_digit_bits(self, bits: int):
+        self.set_tuning(sort_digit_bits=bits)
+
     def set_stream(self, cuda_stream_ptr: int):
         self._ck(self._L.gpsb_set_stream(self._r, C.c_void_p(cuda_stream_ptr) if cuda_stream_ptr else None))
 

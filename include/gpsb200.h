@@ -247,6 +247,22 @@ gpsb_status gpsb_debug_read_subpixels(gpsb_renderer* r, uint32_t slot, uint64_t*
 /* Device-side error word (bounded waits that gave up); 0 when healthy. */
 uint32_t gpsb_debug_error_word(gpsb_renderer* r);
 
+/* Launch-shape tuning (no reference counterpart). Zero fields keep the current value.
+ *   sort_digit_bits        radix digit width of the depth sort: 4, 6 or 8 (default 8)
+ *   blend_tile_w/h         screen tiles of the sorted blend: 16x16 (default), 32x8 or 32x32
+ *   particle_items         particles per thread per tile of the particle kernel: 8 (default), 16, 24
+ *   particle_blocks_per_sm persistent grid of the particle kernel (default 4)
+ *   ensemble_batch         most ensembles per device batch (default 64, at most 1024) */
+typedef struct gpsb_tuning {
+    uint32_t sort_digit_bits;
+    uint32_t blend_tile_w, blend_tile_h;
+    uint32_t particle_items;
+    uint32_t particle_blocks_per_sm;
+    uint32_t ensemble_batch;
+} gpsb_tuning;
+gpsb_status gpsb_set_tuning(gpsb_renderer* r, const gpsb_tuning* t);
+gpsb_status gpsb_get_tuning(const gpsb_renderer* r, gpsb_tuning* out);
+
 /* Stage timing: enable (1) or disable (0) CUDA-event timing of every stage; both reset the
  * profile. Launch counting is always on. */
 gpsb_status gpsb_profile_enable(gpsb_renderer* r, int enable);
