@@ -105,9 +105,12 @@ constexpr float kTwoOverPi = 0.636619747f;
 GX_HD float pow2i(int k) { return b2f((uint32_t)(k + 127) << 23); }
 
 GX_HD float exp(float x) {
-    if (x != x) return x;
-    if (x > 88.7228394f) return b2f(0x7F800000u);
-    if (x < -103.972084f) return 0.0f;
+    // one range test: NaN, overflow and the subnormal/underflow tail take the slow branch
+    if (!(x >= -87.3365479f && x <= 88.7228394f)) {
+        if (x != x) return x;
+        if (x > 88.7228394f) return b2f(0x7F800000u);
+        if (x < -103.972084f) return 0.0f;
+    }
     float kf = rint_(x * kLog2e);
     float r = fma_(kf, -kLn2Hi, x);
     r = fma_(kf, -kLn2Lo, r);
@@ -121,19 +124,19 @@ GX_HD float exp(float x) {
     p = fma_(p, r, 1.0f);
     p = fma_(p, r, 1.0f);
     int k = (int)kf;
+    if (k >= -126 && k <= 127) return p * pow2i(k);
     if (k > 127) return (p * 2.0f) * pow2i(k - 1);
-    if (k < -126) return (p * pow2i(k + 64)) * pow2i(-64);
-    return p * pow2i(k);
+    return (p * pow2i(k + 64)) * pow2i(-64);
 }
 
 GX_HD float log(float x) {
-    if (x != x || x < 0.0f) return b2f(0x7FC00000u);
-    if (x == 0.0f) return b2f(0xFF800000u);
-    if (x == b2f(0x7F800000u)) return x;
     uint32_t b = f2b(x);
     int e = 0;
-    if (b < 0x00800000u) {  // subnormal: scale into the normal range (exact)
-        x = x * 8388608.0f;
+    if (b - 0x00800000u >= 0x7F000000u) {  // one test: zero, subnormal, negative, infinite or NaN
+        if (x != x || x < 0.0f) return b2f(0x7FC00000u);
+        if (x == 0.0f) return b2f(0xFF800000u);
+        if (b == 0x7F800000u) return x;
+        x = x * 8388608.0f;  // subnormal: scale into the normal range (exact)
         b = f2b(x);
         e = -23;
     }
@@ -182,14 +185,12 @@ GX_HD void sincos(float x, float* s, float* c) {
     float r = fma_(kf, -kPio2Hi, x);
     r = fma_(kf, -kPio2Lo, r);
     float sp = sin_poly(r), cp = cos_poly(r);
-    int q = ((int)kf) & 3;
-    float so, co;
-    if (q == 0) { so = sp; co = cp; }
-    else if (q == 1) { so = cp; co = -sp; }
-    else if (q == 2) { so = -sp; co = -cp; }
-    else { so = -cp; co = sp; }
-    *s = so;
-    *c = co;
+    // quadrant q: odd q swaps sin and cos; sin is negated for q = 2, 3 and cos for q = 1, 2
+    uint32_t q = (uint32_t)(int)kf;
+    float so = (q & 1u) ? cp : sp;
+    float co = (q & 1u) ? sp : cp;
+    *s = b2f(f2b(so) ^ ((q & 2u) << 30));
+    *c = b2f(f2b(co) ^ (((q + 1u) & 2u) << 30));
 }
 GX_HD float sin(float x) { float s, c; sincos(x, &s, &c); return s; }
 GX_HD float cos(float x) { float s, c; sincos(x, &s, &c); return c; }

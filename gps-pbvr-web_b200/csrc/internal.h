@@ -23,6 +23,7 @@ struct FrameConst {
     float bg[3];
     uint32_t method, calibration, flags, sh_deg;
     float base_k, refl, object_depth;
+    float jitter_sd;       // sqrt(max(low_pass, 0)), the low-pass jitter scale (gps_splat.wgsl:507)
 };
 
 enum : uint32_t { FLAG_RADIAL = 1u, FLAG_CENTRE = 2u, FLAG_JITTER = 4u };

@@ -12,6 +12,11 @@
 
 #include "devmath.cuh"
 
+// Resident blocks per SM the particle kernel is compiled for (register budget).
+#ifndef GPSB_PARTICLE_MIN_BLOCKS
+#define GPSB_PARTICLE_MIN_BLOCKS 5
+#endif
+
 namespace gpsb {
 
 typedef unsigned long long ull;
@@ -404,9 +409,8 @@ __device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, uint32_t i, u
     if (flags & FLAG_JITTER) {
         float jy = nm.next();
         float jx = nm.next();
-        float sj = sqrt_(fmax_(f.low_pass, F_(0.0)));
-        pix_x = pix_x + sj * jx;
-        pix_y = pix_y + sj * jy;
+        pix_x = pix_x + f.jitter_sd * jx;
+        pix_y = pix_y + f.jitter_sd * jy;
     }
     float4 r0 = R[0];
     if (flags & FLAG_RADIAL) {
@@ -480,7 +484,7 @@ __device__ __forceinline__ uint32_t warp_last_le(const uint2* __restrict__ L, ui
 // with one 64-bit atomicMin of (depth key << 32 | i), which equals the reference's depth pass
 // followed by the colour pass (gps_splat.wgsl:276-281). Ensembles flagged skipped get no work.
 template <int MC, int kPIPT>  // MC: 0 GPS, 1 PBVR, 2 ScreenOccupancy; kPIPT: particles per thread per tile
-__global__ void __launch_bounds__(kPT) k_particles(FrameConst f, const float4* __restrict__ rec,
+__global__ void __launch_bounds__(kPT, GPSB_PARTICLE_MIN_BLOCKS) k_particles(FrameConst f, const float4* __restrict__ rec,
                                                    const float* __restrict__ lut, const uint2* __restrict__ clist,
                                                    const EnsTotal* __restrict__ etot, uint32_t first_seed, uint32_t E,
                                                    ull* sub, uint32_t* unit_counter, ull* stats) {

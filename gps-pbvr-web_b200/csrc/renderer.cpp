@@ -4,6 +4,7 @@
 // on one stream; render calls enqueue work and return (like queue.submit), readbacks wait.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <math.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -93,7 +94,7 @@ struct gpsb_renderer {
     double ms[GPSB_STAGES] = {};
     uint64_t total_launches = 0;
     // launch-shape tuning
-    uint32_t particle_items = 8, particle_blocks_per_sm = 4, ensemble_batch = 64;
+    uint32_t particle_items = 16, particle_blocks_per_sm = 5, ensemble_batch = 64;
 };
 
 // Brackets the kernels of one stage with CUDA events on the renderer's stream (when profiling)
@@ -163,6 +164,7 @@ static FrameConst make_frame(const gpsb_renderer* r, const gpsb_camera& cam, con
         f.pos[k] = (float)cam.view_pos[k];
     }
     f.low_pass = (float)cam.low_pass;
+    f.jitter_sd = sqrtf(fmaxf(f.low_pass, 0.0f));
     double cx = cam.cx, cy = cam.cy;
     if (cam.cx == 0.0 && cam.cy == 0.0) {  // gps.rs:818
         cx = 0.5 * r->W;

@@ -250,8 +250,8 @@ uint32_t gpsb_debug_error_word(gpsb_renderer* r);
 /* Launch-shape tuning (no reference counterpart). Zero fields keep the current value.
  *   sort_digit_bits        radix digit width of the depth sort: 4, 6 or 8 (default 8)
  *   blend_tile_w/h         screen tiles of the sorted blend: 16x16 (default), 32x8 or 32x32
- *   particle_items         particles per thread per tile of the particle kernel: 8 (default), 16, 24
- *   particle_blocks_per_sm persistent grid of the particle kernel (default 4)
+ *   particle_items         particles per thread per tile of the particle kernel: 8, 16 (default), 24
+ *   particle_blocks_per_sm persistent grid of the particle kernel (default 5 per SM)
  *   ensemble_batch         most ensembles per device batch (default 64, at most 1024) */
 typedef struct gpsb_tuning {
     uint32_t sort_digit_bits;

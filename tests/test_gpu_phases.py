@@ -284,7 +284,7 @@ def test_phase4_sh_degrees_vs_eval_sh():
 
 
 # ------------------------------------------------------------------ launch shapes never change results
-@pytest.mark.parametrize("tune", [dict(particle_items=16), dict(particle_items=24), dict(particle_blocks_per_sm=1),
+@pytest.mark.parametrize("tune", [dict(particle_items=8), dict(particle_items=24), dict(particle_blocks_per_sm=1),
                                   dict(particle_blocks_per_sm=8), dict(ensemble_batch=3)])
 def test_tuning_does_not_change_results(tune):
     items = SCENES[4][1]
