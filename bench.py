@@ -237,7 +237,9 @@ def run_b200(args, rank, world):
     r = pkg.GpsRenderer(W, H, SIDE, device=dev)
     r.set_stream(stream.cuda_stream)
     r.set_gaussians_sh(splats, sh, deg)
-    seed0 = 1 + rank * 1_000_003
+    from gps_pbvr_web_b200 import multi
+    # weak scaling: every rank renders ENS ensembles per view; the ranks' seeds are disjoint
+    seed0 = multi.rank_first_seed(1, world * ENS, world, rank)
 
     def step(seed):
         for _, cam in cams:
@@ -268,10 +270,7 @@ def run_b200(args, rank, world):
     ms = t_start.elapsed_time(t_end)
     prof = r.profile()
     st = r.read_stats()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = multi.max_over_ranks(ms, dist, device="cuda")
     ens_total = world * args.steps * len(cams) * ENS
     value = ens_total / (ms / 1000.0)
 
@@ -339,10 +338,7 @@ def run_b200(args, rank, world):
             e2e_step()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([dt], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = multi.max_over_ranks(dt, dist, device="cuda")
         e2e = {"value": world * e_steps * len(cams) * ENS / dt, "unit": "ensembles/s",
                "h2d_bytes_per_step": int(splats.nbytes + sh.nbytes), "d2h_bytes_per_step": int(len(cams) * P * 16),
                "steps": e_steps, "timing": "host wall clock around synchronised steps"}
