@@ -219,6 +219,73 @@ def algorithmic_bytes_per_launch(stage, writes, entries, E, n_splats, P):
     return 0.0
 
 
+def micro_scan_sort(pkg, r, stream, peak):
+    """HBM throughput of the two data-movement primitives at sizes far above L2:
+    exclusive scan of 2^28 u32 counts (8 algorithmic bytes per element: read + write) and the
+    stable radix sort of 2^26 (24-bit key, value) pairs with 8-bit digits (4 bytes of histogram read
+    + 3 passes x 16 bytes of key/value read and write = 52 bytes per pair)."""
+    import ctypes as C
+    import torch
+    L = pkg.abi.lib()
+    out = {}
+    n = 1 << 28
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.randint(0, 16, (n,), dtype=torch.int32, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+    def scan():
+        assert L.gpsb_scan_u32(r.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), n, C.c_void_p(tot.data_ptr())) == 0
+    ms = _time_events(scan, stream, 3, 10)
+    out["scan_u32"] = {"n": n, "ms": ms, "alg_bytes": 8 * n, "GBps": 8 * n / (ms / 1e3) / 1e9,
+                       "frac": 8 * n / (ms / 1e3) / 1e9 / peak}
+    del x, y
+    n = 1 << 26
+    keys = torch.randint(0, 1 << 24, (n,), dtype=torch.int32, device="cuda", generator=g)
+    vals = torch.arange(n, dtype=torch.int32, device="cuda")
+    ka, va, kb, vb = keys.clone(), vals.clone(), torch.empty_like(keys), torch.empty_like(vals)
+    for bits in (8, 6, 4):
+        r.set_tuning(sort_digit_bits=bits)
+        passes = -(-24 // bits)
+        def sort():
+            ka.copy_(keys)
+            va.copy_(vals)
+        def run():
+            assert L.gpsb_sort_pairs(r.handle, C.c_void_p(ka.data_ptr()), C.c_void_p(va.data_ptr()),
+                                     C.c_void_p(kb.data_ptr()), C.c_void_p(vb.data_ptr()), n, 24) == 0
+        # inputs are clobbered by the ping-pong passes: restore them outside the timed region
+        tms = []
+        for k in range(6):
+            sort()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            run()
+            b.record(stream)
+            torch.cuda.synchronize()
+            if k >= 2:
+                tms.append(a.elapsed_time(b))
+        ms = statistics.median(tms)
+        alg = (4 + 16 * passes + (8 if passes % 2 == 0 else 0)) * n
+        out[f"sort_pairs_{bits}bit"] = {"n": n, "ms": ms, "alg_bytes": alg, "GBps": alg / (ms / 1e3) / 1e9,
+                                        "frac": alg / (ms / 1e3) / 1e9 / peak}
+    r.set_tuning(sort_digit_bits=8)
+    return out
+
+
+def _time_events(fn, stream, warmup, reps):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
 def run_b200(args, rank, world):
     import torch
     pkg = load_package()
@@ -343,6 +410,10 @@ def run_b200(args, rank, world):
                "h2d_bytes_per_step": int(splats.nbytes + sh.nbytes), "d2h_bytes_per_step": int(len(cams) * P * 16),
                "steps": e_steps, "timing": "host wall clock around synchronised steps"}
 
+    prims = None
+    if rank == 0 and not args.no_micro:
+        prims = micro_scan_sort(pkg, r, stream, peak)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cams = cameras(pkg)
@@ -370,7 +441,7 @@ def run_b200(args, rank, world):
                                    "list_entries": st.list_entries / args.steps,
                                    "truncated_splats": st.truncated_splats / args.steps,
                                    "skipped_ensembles": st.skipped_ensembles},
-                "e2e": e2e, "cpu_baseline": cpu}
+                "primitives": prims, "e2e": e2e, "cpu_baseline": cpu}
         print(json.dumps(line))
     r.close()
     if dist is not None:
@@ -387,6 +458,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-micro", action="store_true", help="skip the scan/sort HBM measurements")
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64)
     ap.add_argument("--views", default="near,mid,far", help="subset of the views (small profiling cases)")
     ap.add_argument("--ensembles", type=int, default=ENS, help="ensembles per view (small profiling cases)")

@@ -108,6 +108,9 @@ SIGNATURES = {
     "gpsb_profile_read": (ST, [P, P]),
     "gpsb_sort_pairs_noalloc": (ST, [P, P, P, P, U32, U32, P, P]),
     "gpsb_set_tuning": (ST, [P, P]),
+    "gpsb_scan_u32": (ST, [P, P, P, U32, P]),
+    "gpsb_sort_pairs": (ST, [P, P, P, P, P, U32, U32]),
+    "gpsb_p0_sample": (ST, [P, U32, U32, U32, U32, P]),
     "gpsb_get_tuning": (ST, [P, P]),
 }
 

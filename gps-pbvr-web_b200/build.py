@@ -22,7 +22,7 @@ CU_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler
                    "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-I" + os.path.join(CUDA, "include"),
              "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
-LIB_SOURCES = ["kernels.cu", "sorted.cu", "renderer.cpp", "hostmath.cpp", "ply.cpp"]
+LIB_SOURCES = ["kernels.cu", "sorted.cu", "primitives.cu", "renderer.cpp", "hostmath.cpp", "ply.cpp"]
 
 
 def _headers():

@@ -94,6 +94,13 @@ struct SortedBuffers;
 void launch_composite(const float4* accum, uint32_t W, uint32_t H, float exposure, uint32_t gamma_on, uint32_t out_w,
                       uint32_t out_h, uchar4* out, cudaStream_t st);
 
+// stand-alone primitives (primitives.cu)
+uint32_t scan_tiles(uint32_t n);
+void launch_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint64_t* lookback, uint32_t* counter,
+                     uint64_t* total, uint32_t* err, cudaStream_t st);
+void launch_p0_sample(uint32_t seed, uint32_t pixel_base, uint32_t pixels, uint32_t samples, unsigned long long* packed,
+                      cudaStream_t st);
+
 int device_sm_count(int device);
 
 }  // namespace gpsb

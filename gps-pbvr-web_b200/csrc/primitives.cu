@@ -1,0 +1,170 @@
+// Stand-alone primitives of the hot path, for the Phase-0 checks of the reference
+// (crates/gps-render/src/lib.rs:99-275) and for HBM roofline measurements:
+//   k_scan_u32    single-pass decoupled-lookback exclusive scan of u32 counts (replaces the
+//                 hierarchical scan_block/add_offsets of shaders/gps_scan.wgsl), 64-bit total;
+//   k_p0_sample   the synthetic two-pass atomicMin check of shaders/p0_sample.wgsl, with the
+//                 packed 64-bit (key << 32 | colour) atomicMin that the particle kernel uses.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace gpsb {
+
+typedef unsigned long long ull;
+
+constexpr int kSThreads = 256;
+constexpr int kSItems = 16;
+constexpr int kSTile = kSThreads * kSItems;
+constexpr uint64_t kSAgg = 1ull << 62, kSPre = 2ull << 62, kSMask = (1ull << 62) - 1ull;
+
+__device__ __forceinline__ uint64_t ld_rlx(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_rlx(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Each block scans kSTile consecutive counts (16 per thread, two 128-bit loads), publishes its
+// aggregate, looks back over its predecessors (warp 0, 32 at a time) and writes the exclusive
+// prefix; the last tile writes the 64-bit total. Tile indices come from an atomic counter so
+// every predecessor is running or done; waits are bounded and report through *err.
+__global__ void __launch_bounds__(kSThreads) k_scan_u32(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                       uint32_t n, uint64_t* lookback, uint32_t* tile_counter,
+                                                       uint32_t* err) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint64_t s_w[kSThreads / 32];
+    __shared__ uint64_t s_excl;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    const uint32_t base = t * kSTile + tid * kSItems;
+    uint32_t v[kSItems];
+    if (base + kSItems <= n && (((uintptr_t)(in + base)) & 15u) == 0) {
+#pragma unroll
+        for (int q = 0; q < kSItems; q += 4) {
+            uint4 x = __ldcs(reinterpret_cast<const uint4*>(in + base + q));
+            v[q] = x.x; v[q + 1] = x.y; v[q + 2] = x.z; v[q + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < kSItems; ++q) v[q] = base + q < n ? in[base + q] : 0u;
+    }
+    uint64_t tsum = 0;
+#pragma unroll
+    for (int q = 0; q < kSItems; ++q) tsum += v[q];
+    uint64_t incl = tsum;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t a = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += a;
+    }
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    uint64_t wpre = 0, agg = 0;
+#pragma unroll
+    for (int w = 0; w < kSThreads / 32; ++w) {
+        if (w < warp) wpre += s_w[w];
+        agg += s_w[w];
+    }
+    if (warp == 0) {
+        uint64_t excl = 0;
+        if (t == 0) {
+            if (lane == 0) st_rlx(&lookback[0], kSPre | agg);
+        } else {
+            if (lane == 0) st_rlx(&lookback[t], kSAgg | agg);
+            int32_t pred = (int32_t)t - 1;
+            uint32_t spins = 0;
+            bool failed = false;
+            while (true) {
+                int32_t j = pred - lane;
+                uint64_t w = kSPre;
+                if (j >= 0) {
+                    w = ld_rlx(&lookback[j]);
+                    while ((w >> 62) == 0ull) {
+                        if (++spins > (1u << 20)) { failed = true; break; }
+                        __nanosleep(64);
+                        w = ld_rlx(&lookback[j]);
+                    }
+                }
+                if (__any_sync(0xffffffffu, failed)) { failed = true; break; }
+                uint32_t pre = __ballot_sync(0xffffffffu, (w >> 62) == 2ull);
+                int first = pre ? __ffs(pre) - 1 : 32;
+                uint64_t val = lane <= first ? (w & kSMask) : 0ull;
+                for (int o = 16; o; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+                excl += val;
+                if (first < 32) break;
+                pred -= 32;
+            }
+            if (failed && lane == 0) atomicOr(err, ERR_SCAN_LOOKBACK);
+            if (lane == 0) st_rlx(&lookback[t], kSPre | ((excl + agg) & kSMask));
+        }
+        if (lane == 0) s_excl = excl;
+    }
+    __syncthreads();
+    uint64_t run = s_excl + wpre + (incl - tsum);
+    uint32_t o[kSItems];
+#pragma unroll
+    for (int q = 0; q < kSItems; ++q) {
+        o[q] = (uint32_t)run;
+        run += v[q];
+    }
+    if (base + kSItems <= n && (((uintptr_t)(out + base)) & 15u) == 0) {
+#pragma unroll
+        for (int q = 0; q < kSItems; q += 4)
+            __stcs(reinterpret_cast<uint4*>(out + base + q), make_uint4(o[q], o[q + 1], o[q + 2], o[q + 3]));
+    } else {
+#pragma unroll
+        for (int q = 0; q < kSItems; ++q)
+            if (base + q < n) out[base + q] = o[q];
+    }
+}
+
+// The total is the inclusive prefix published by the last tile (status bits cleared).
+__global__ void k_scan_total(uint64_t* total, const uint64_t* lookback, uint32_t tiles) {
+    *total = lookback[tiles - 1] & kSMask;
+}
+
+uint32_t scan_tiles(uint32_t n) { return (n + kSTile - 1) / kSTile; }
+
+void launch_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint64_t* lookback, uint32_t* counter,
+                     uint64_t* total, uint32_t* err, cudaStream_t st) {
+    uint32_t tiles = scan_tiles(n);
+    cudaMemsetAsync(lookback, 0, (size_t)(tiles ? tiles : 1) * 8, st);
+    cudaMemsetAsync(counter, 0, 4, st);
+    if (n == 0) {
+        if (total) cudaMemsetAsync(total, 0, 8, st);
+        return;
+    }
+    k_scan_u32<<<tiles, kSThreads, 0, st>>>(in, out, n, lookback, counter, err);
+    if (total) k_scan_total<<<1, 1, 0, st>>>(total, lookback, tiles);
+}
+
+// p0_sample.wgsl:26-39 gen_sample: pixel, ordered depth key (deliberately few values) and colour
+__device__ __forceinline__ void p0_sample(uint32_t seed, uint32_t pixel_base, uint32_t pixels, uint32_t i, uint32_t* pix,
+                                          uint32_t* key, uint32_t* rgb) {
+    uint32_t h0 = gx::pcg(i ^ gx::pcg(seed));
+    uint32_t h1 = gx::pcg(h0);
+    uint32_t h2 = gx::pcg(h1);
+    *pix = pixel_base + (h0 % pixels);
+    uint32_t bits = 0x3F800000u | (h1 & 0x007FFFFFu);
+    *key = (bits | 0x80000000u) & 0xFFFF0000u;
+    *rgb = h2 & 0x00FFFFFFu;
+}
+
+__global__ void k_p0_sample(uint32_t seed, uint32_t pixel_base, uint32_t pixels, uint32_t samples, ull* packed) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= samples) return;
+    uint32_t pix, key, rgb;
+    p0_sample(seed, pixel_base, pixels, i, &pix, &key, &rgb);
+    atomicMin(packed + pix, ((ull)key << 32) | rgb);
+}
+
+void launch_p0_sample(uint32_t seed, uint32_t pixel_base, uint32_t pixels, uint32_t samples, ull* packed, cudaStream_t st) {
+    if (samples == 0) return;
+    k_p0_sample<<<(samples + 255) / 256, 256, 0, st>>>(seed, pixel_base, pixels, samples, packed);
+}
+
+}  // namespace gpsb

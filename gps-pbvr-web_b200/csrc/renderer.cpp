@@ -93,6 +93,9 @@ struct gpsb_renderer {
     uint64_t launches[GPSB_STAGES] = {};
     double ms[GPSB_STAGES] = {};
     uint64_t total_launches = 0;
+    // stand-alone primitives
+    DevBuf prim_lookback, prim_counter;
+    RadixScratch prim_sort;
     // launch-shape tuning
     uint32_t particle_items = 16, particle_blocks_per_sm = 5, ensemble_batch = 64;
 };
@@ -443,6 +446,9 @@ void gpsb_destroy(gpsb_renderer* r) {
                       &r->sub, &r->clist, &r->lookback, &r->etot, &r->counters, &r->rgba8};
     for (DevBuf* b : bufs) b->release();
     sorted_release(r->sorted);
+    r->prim_lookback.release();
+    r->prim_counter.release();
+    radix_release(r->prim_sort);
     for (auto& pe : r->pending) {
         cudaEventDestroy(pe.a);
         cudaEventDestroy(pe.b);
@@ -779,6 +785,44 @@ gpsb_status gpsb_debug_read_subpixels(gpsb_renderer* r, uint32_t slot, uint64_t*
     CK(r, cudaMemcpyAsync(packed, r->sub.as<uint64_t>() + (size_t)slot * PS, PS * 8, cudaMemcpyDeviceToHost, r->stream),
        "read subpixels");
     CK(r, cudaStreamSynchronize(r->stream), "synchronise");
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_scan_u32(gpsb_renderer* r, const uint32_t* in, uint32_t* out, uint32_t n, uint64_t* total) {
+    if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
+    if (n && (!in || !out)) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null buffer");
+    cudaSetDevice(r->device);
+    CK(r, r->prim_lookback.ensure((size_t)std::max(scan_tiles(n), 1u) * 8), "scan lookback");
+    CK(r, r->prim_counter.ensure(16), "scan counter");
+    launch_scan_u32(in, out, n, r->prim_lookback.as<uint64_t>(), r->prim_counter.as<uint32_t>(), total,
+                    r->err.as<uint32_t>(), r->stream);
+    r->total_launches += 2;
+    CK(r, cudaGetLastError(), "scan kernel");
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_sort_pairs(gpsb_renderer* r, uint32_t* ki, uint32_t* vi, uint32_t* ko, uint32_t* vo, uint32_t n,
+                            uint32_t key_bits) {
+    if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
+    if (key_bits < 1 || key_bits > 32) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "key_bits must be 1..32");
+    if (n && (!ki || !vi || !ko || !vo)) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null buffer");
+    if (n > (1u << 30)) return fail(r, GPSB_ERR_LIMIT, "at most 2^30 pairs");
+    cudaSetDevice(r->device);
+    cudaError_t e = radix_sort_pairs(r->prim_sort, ki, vi, ko, vo, n, (int)key_bits, r->sorted.digit_bits,
+                                     r->err.as<uint32_t>(), r->stream);
+    if (e != cudaSuccess) return cuda_fail(r, e, "radix sort");
+    r->total_launches += 2 + (key_bits + r->sorted.digit_bits - 1) / r->sorted.digit_bits;
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_p0_sample(gpsb_renderer* r, uint32_t seed, uint32_t pixel_base, uint32_t pixels, uint32_t samples,
+                           uint64_t* packed) {
+    if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
+    if (samples && (!packed || pixels == 0)) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null buffer or no pixels");
+    cudaSetDevice(r->device);
+    launch_p0_sample(seed, pixel_base, pixels, samples, (unsigned long long*)packed, r->stream);
+    r->total_launches += 1;
+    CK(r, cudaGetLastError(), "p0 sample kernel");
     return GPSB_OK;
 }
 

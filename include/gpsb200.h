@@ -269,6 +269,24 @@ gpsb_status gpsb_profile_enable(gpsb_renderer* r, int enable);
 /* Reads the profile (synchronises the renderer's stream). */
 gpsb_status gpsb_profile_read(gpsb_renderer* r, gpsb_profile* out);
 
+/* ------------------------------------------------------------------- primitives */
+/* Exclusive scan of n u32 counts (device pointers) on the renderer's stream: the single-pass
+ * decoupled-lookback scan that replaces the hierarchical scan of shaders/gps_scan.wgsl (checked
+ * by the reference at n in {1, 255, 256, 257, 65536, 300000, 1000003}, lib.rs:196-275). out may
+ * equal in. The 64-bit total goes to *total_dev when it is not NULL. Enqueues and returns. */
+gpsb_status gpsb_scan_u32(gpsb_renderer* r, const uint32_t* in_dev, uint32_t* out_dev, uint32_t n,
+                          uint64_t* total_dev);
+/* Stable ascending radix sort of n (key, value) pairs on the low key_bits bits, with the digit
+ * width of gpsb_tuning (shaders/gps_sort.wgsl semantics). keys_in/vals_in are clobbered; scratch
+ * belongs to the renderer. Enqueues and returns. */
+gpsb_status gpsb_sort_pairs(gpsb_renderer* r, uint32_t* keys_in, uint32_t* vals_in, uint32_t* keys_out,
+                            uint32_t* vals_out, uint32_t n, uint32_t key_bits);
+/* Phase-0 winner-rule check (shaders/p0_sample.wgsl, lib.rs:99-192): `samples` synthetic samples
+ * of ensemble `seed` written with one packed atomicMin into packed_dev[pixel_base .. +pixels)
+ * (u64 (depth key << 32) | colour; initialise to all ones). Enqueues and returns. */
+gpsb_status gpsb_p0_sample(gpsb_renderer* r, uint32_t seed, uint32_t pixel_base, uint32_t pixels,
+                           uint32_t samples, uint64_t* packed_dev);
+
 /* ------------------------------------------------------------------- sort without allocation */
 /* No counterpart in the reference. Stable ascending LSD radix sort of n (key, value) pairs on
  * the low key_bits bits (1..32, keys must be below 2^key_bits), the onesweep kernels of the
