@@ -13,8 +13,17 @@ namespace gpsb {
 
 typedef unsigned long long ull;
 
-constexpr int kSThreads = 256;
-constexpr int kSItems = 16;
+#ifndef GPSB_SCAN_THREADS
+#define GPSB_SCAN_THREADS 256
+#endif
+#ifndef GPSB_SCAN_ITEMS
+#define GPSB_SCAN_ITEMS 24
+#endif
+#ifndef GPSB_SCAN_SLEEP
+#define GPSB_SCAN_SLEEP 8
+#endif
+constexpr int kSThreads = GPSB_SCAN_THREADS;
+constexpr int kSItems = GPSB_SCAN_ITEMS;  // a multiple of 4: 128-bit loads and stores
 constexpr int kSTile = kSThreads * kSItems;
 constexpr uint64_t kSAgg = 1ull << 62, kSPre = 2ull << 62, kSMask = (1ull << 62) - 1ull;
 
@@ -27,7 +36,7 @@ __device__ __forceinline__ void st_rlx(uint64_t* p, uint64_t v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Each block scans kSTile consecutive counts (16 per thread, two 128-bit loads), publishes its
+// Each block scans kSTile consecutive counts (kSItems per thread, 128-bit loads), publishes its
 // aggregate, looks back over its predecessors (warp 0, 32 at a time) and writes the exclusive
 // prefix; the last tile writes the 64-bit total. Tile indices come from an atomic counter so
 // every predecessor is running or done; waits are bounded and report through *err.
@@ -85,7 +94,7 @@ __global__ void __launch_bounds__(kSThreads) k_scan_u32(const uint32_t* __restri
                     w = ld_rlx(&lookback[j]);
                     while ((w >> 62) == 0ull) {
                         if (++spins > (1u << 20)) { failed = true; break; }
-                        __nanosleep(64);
+                        __nanosleep(GPSB_SCAN_SLEEP);
                         w = ld_rlx(&lookback[j]);
                     }
                 }

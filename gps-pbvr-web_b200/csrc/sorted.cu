@@ -44,7 +44,7 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // ============================================================================ radix sort
 constexpr int kRsThreads = 256;
 constexpr int kRsWarps = kRsThreads / 32;
-constexpr int kRsIpt = 15;
+constexpr int kRsIpt = 15;  // keys per thread: 3840 per tile, 30 KB of shared staging
 constexpr int kRsTile = kRsThreads * kRsIpt;
 constexpr int kMaxPasses = 8;
 constexpr uint32_t kStAgg = 1u << 30, kStPre = 2u << 30, kStMask = (1u << 30) - 1u;
@@ -85,17 +85,24 @@ __global__ void __launch_bounds__(kRsThreads) k_onesweep(const uint32_t* __restr
                                                          uint32_t n, int shift, const uint32_t* __restrict__ gstart,
                                                          uint32_t* lookback, uint32_t* tile_counter, uint32_t* err) {
     constexpr int BINS = 1 << BITS;
-    __shared__ uint32_t s_wcnt[kRsWarps][BINS];
-    __shared__ uint32_t s_base[BINS];
+    __shared__ uint32_t s_wcnt[kRsWarps][BINS];  // per-warp digit counts, then exclusive prefix over warps
+    __shared__ uint32_t s_dstart[BINS];          // tile-local exclusive prefix over digits
+    __shared__ uint32_t s_gbase[BINS];           // global position of the digit's first key of this tile, minus s_dstart
+    __shared__ uint32_t s_key[kRsTile];
+    __shared__ uint32_t s_val[kRsTile];
+    __shared__ uint32_t s_wsum[kRsWarps];
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
     for (int k = tid; k < kRsWarps * BINS; k += kRsThreads) (&s_wcnt[0][0])[k] = 0;
     __syncthreads();
     const uint32_t t = s_tile;
-    const uint32_t base = t * kRsTile + warp * 32 * kRsIpt;
+    const uint32_t tile0 = t * kRsTile;
+    const uint32_t tile_n = n - tile0 < (uint32_t)kRsTile ? n - tile0 : (uint32_t)kRsTile;
+    const uint32_t base = tile0 + warp * 32 * kRsIpt;
     uint32_t key[kRsIpt], val[kRsIpt], rank[kRsIpt];
     const uint32_t lt = lanemask_lt();
+    // rank every key within its warp's sub-tile in input order (stable): warp-match on the digit
 #pragma unroll
     for (int q = 0; q < kRsIpt; ++q) {
         uint32_t idx = base + q * 32 + lane;
@@ -111,27 +118,49 @@ __global__ void __launch_bounds__(kRsThreads) k_onesweep(const uint32_t* __restr
         __syncwarp();
     }
     __syncthreads();
-    // per digit: exclusive prefix over warps (stable: warps own consecutive sub-tiles), then
-    // a decoupled lookback over the tiles for the digit's global offset
+    // per digit: exclusive prefix over warps and the tile count; publish the tile's aggregate early
     uint32_t* lb = lookback + (size_t)t * BINS;
-    for (int d = tid; d < BINS; d += kRsThreads) {
-        uint32_t run = 0;
+    uint32_t cnt = 0;
+    if (tid < BINS) {
 #pragma unroll
         for (int w = 0; w < kRsWarps; ++w) {
-            uint32_t c = s_wcnt[w][d];
-            s_wcnt[w][d] = run;
-            run += c;
+            uint32_t c = s_wcnt[w][tid];
+            s_wcnt[w][tid] = cnt;
+            cnt += c;
         }
+        st_relaxed32(&lb[tid], (t == 0 ? kStPre : kStAgg) | cnt);
+    }
+    // exclusive scan of the digit counts over the tile (BINS <= 256 = one value per thread)
+    uint32_t incl = tid < BINS ? cnt : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t a = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += a;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += s_wsum[w];
+    if (tid < BINS) s_dstart[tid] = wbase + incl - cnt;
+    __syncthreads();
+    // scatter into shared memory in digit order (stable), then resolve the global offsets
+#pragma unroll
+    for (int q = 0; q < kRsIpt; ++q) {
+        uint32_t idx = base + q * 32 + lane;
+        if (idx < n) {
+            uint32_t d = (key[q] >> shift) & (BINS - 1);
+            uint32_t pos = s_dstart[d] + s_wcnt[warp][d] + rank[q];
+            s_key[pos] = key[q];
+            s_val[pos] = val[q];
+        }
+    }
+    if (tid < BINS) {
         uint32_t excl = 0;
-        if (t == 0) {
-            st_relaxed32(&lb[d], kStPre | run);
-        } else {
-            st_relaxed32(&lb[d], kStAgg | run);
+        if (t > 0) {
             int32_t pred = (int32_t)t - 1;
             uint32_t spins = 0;
             bool failed = false;
             while (pred >= 0) {
-                uint32_t w = ld_relaxed32(&lookback[(size_t)pred * BINS + d]);
+                uint32_t w = ld_relaxed32(&lookback[(size_t)pred * BINS + tid]);
                 if ((w >> 30) == 0u) {
                     if (++spins > (1u << 22)) { failed = true; break; }
                     __nanosleep(32);
@@ -142,23 +171,20 @@ __global__ void __launch_bounds__(kRsThreads) k_onesweep(const uint32_t* __restr
                 --pred;
             }
             if (failed) atomicOr(err, ERR_SORT_LOOKBACK);
-            st_relaxed32(&lb[d], kStPre | ((excl + run) & kStMask));
+            st_relaxed32(&lb[tid], kStPre | ((excl + cnt) & kStMask));
         }
-        s_base[d] = gstart[d] + excl;
+        s_gbase[tid] = gstart[tid] + excl - s_dstart[tid];
     }
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kRsIpt; ++q) {
-        uint32_t idx = base + q * 32 + lane;
-        if (idx < n) {
-            uint32_t d = (key[q] >> shift) & (BINS - 1);
-            uint32_t pos = s_base[d] + s_wcnt[warp][d] + rank[q];
-            if (pos < n) {
-                kout[pos] = key[q];
-                vout[pos] = val[q];
-            } else {
-                atomicOr(err, ERR_BAD_INDEX);
-            }
+    // coalesced write-out: consecutive threads write consecutive keys of each digit run
+    for (uint32_t i = tid; i < tile_n; i += kRsThreads) {
+        uint32_t k = s_key[i];
+        uint32_t pos = s_gbase[(k >> shift) & (BINS - 1)] + i;
+        if (pos < n) {
+            kout[pos] = k;
+            vout[pos] = s_val[i];
+        } else {
+            atomicOr(err, ERR_BAD_INDEX);
         }
     }
 }

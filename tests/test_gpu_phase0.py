@@ -85,6 +85,36 @@ def test_scan_sizes(n):
     r.close()
 
 
+@pytest.mark.parametrize("n,offset,full", [(524288, 0, False), (524288 + 8192 * 3 + 5, 0, False),
+                                           (4_000_001, 0, False), (600_000, 0, True), (1_000_003, 1, False),
+                                           (1_000_003, 2, True)])
+def test_scan_large_paths(n, offset, full):
+    """Sizes that take the persistent bulk-copy scan (16-byte aligned, n >= 2^19) with ragged
+    tails, full-range u32 counts whose total passes 2^32, and misaligned views that take the
+    per-tile kernel instead."""
+    import torch
+    dev = torch.device("cuda", 0)
+    h = _pcg(np.arange(n, dtype=np.uint32) + np.uint32(offset * 77))
+    x = h if full else (h % 13).astype(np.uint32)
+    buf = torch.zeros(n + offset, dtype=torch.int32, device=dev)
+    buf[offset:] = torch.from_numpy(x.view(np.int32))
+    t_in = buf[offset:]
+    obuf = torch.zeros(n + offset, dtype=torch.int32, device=dev)
+    t_out = obuf[offset:]
+    total = torch.zeros(1, dtype=torch.int64, device=dev)
+    r = _renderer()
+    L = PKG.abi.lib()
+    assert L.gpsb_scan_u32(r.handle, C.c_void_p(t_in.data_ptr()), C.c_void_p(t_out.data_ptr()), n,
+                           C.c_void_p(total.data_ptr())) == 0
+    r.wait_idle()
+    cs = np.cumsum(x.astype(np.uint64))
+    ref = np.concatenate([[0], cs[:-1]]).astype(np.uint64) & np.uint64(0xFFFFFFFF)
+    assert np.array_equal(t_out.cpu().numpy().view(np.uint32), ref.astype(np.uint32))
+    assert int(total.item()) == int(cs[-1])
+    assert r.debug_error_word() == 0
+    r.close()
+
+
 def test_scan_full_size_properties():
     import torch
     dev = torch.device("cuda", 0)
