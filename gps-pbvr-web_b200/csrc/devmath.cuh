@@ -19,6 +19,27 @@ using gx::fmin_;
 using gx::sqrt_;
 
 // ----------------------------------------------------------------------------- shared maths
+// Bases of the fmath tables (log, exp, sin/cos) a kernel reads: shared-memory copies in the
+// particle kernel, the global copies elsewhere; both hold the same values.
+struct FTabs {
+    const float* lg;
+    const float* ex;
+    const float* sc;
+};
+constexpr int kTabFloats = gx::kScNodes * 4 + gx::kLogNodes * 4 + gx::kExpNodes * 2;  // staged table floats
+
+// Copies the tables into shared memory at s (16-byte aligned, kTabFloats floats) and returns
+// their bases; the caller synchronises the block before the first use.
+__device__ __forceinline__ FTabs stage_tabs(float* s) {
+    for (int k = threadIdx.x; k < kTabFloats; k += blockDim.x) {
+        float v;
+        if (k < gx::kScNodes * 4) v = gx::kScTabD[k];
+        else if (k < gx::kScNodes * 4 + gx::kLogNodes * 4) v = gx::kLogTabD[k - gx::kScNodes * 4];
+        else v = gx::kExpTabD[k - gx::kScNodes * 4 - gx::kLogNodes * 4];
+        s[k] = v;
+    }
+    return FTabs{s + gx::kScNodes * 4, s + gx::kScNodes * 4 + gx::kLogNodes * 4, s};
+}
 struct Proj {
     bool ok;
     float mx, my, a, b, c, depth;
@@ -124,8 +145,9 @@ __device__ inline float corrected_radius_exact(float o, float li2o, float u) {
 }
 __device__ __forceinline__ float mix_(float a, float b, float t) { return a * (F_(1.0) - t) + b * t; }
 // corrected_radius_lut (gps_splat.wgsl:117-130) with the o-row (i0, a) hoisted per splat
-__device__ __forceinline__ float corrected_radius_lut(const float* lut, uint32_t i0, float a, float u) {
-    float v = -gx::log(fmax_(F_(1.0) - u, gxc::kUMin));
+__device__ __forceinline__ float corrected_radius_lut(const float* lut, uint32_t i0, float a, float u,
+                                                     const float* lg = gx::tab_log()) {
+    float v = -gx::log_t(fmax_(F_(1.0) - u, gxc::kUMin), lg);
     float fv = fmin_(sqrt_(v) * gxc::kLutFv, F_(128.0));
     uint32_t j0 = min(f2u(fv), 127u);
     float b = fv - (float)j0;
@@ -166,9 +188,9 @@ __device__ inline float pixel_density_scale(const FrameConst& f, float depth) {
     float ratio = div_(f.refl, depth);
     return fmin_(ratio * ratio * f.fx * f.fy, F_(1.0e12));
 }
-__device__ __forceinline__ float eol(float x) {
+__device__ __forceinline__ float eol(float x, const float* lg = gx::tab_log()) {
     if (x < F_(1e-4)) return F_(1.0) + F_(0.5) * x;
-    return div_(-gx::log(F_(1.0) - fmin_(x, gxc::kOneMinus1e6)), x);
+    return div_(-gx::log_t(F_(1.0) - fmin_(x, gxc::kOneMinus1e6), lg), x);
 }
 
 // splat_colour (gps_splat.wgsl:210-251)

@@ -4,24 +4,31 @@
 // renderer (shaders/gps_splat.wgsl) has no bit-exact CPU twin. This header defines ONE
 // implementation of each transcendental that computes the same bits on the host (g++,
 // -ffp-contract=off) and on the device (nvcc --fmad=false): every step is an IEEE-754
-// correctly rounded +, -, *, /, sqrt or an explicit fused multiply-add, so the result does
-// not depend on the compiler or the processor.
+// correctly rounded +, -, *, /, sqrt, an explicit fused multiply-add or a read of a constant
+// table (fmath_tables.h, exact float32 literals), so the result does not depend on the
+// compiler or the processor.
 //
-// Methods (all from published mathematics, no fitted coefficients):
-//   exp  : Cody & Waite (1980) argument reduction x = k ln2 + r with a two-part ln2 applied by
-//          FMA, |r| <= ln2/2, then the Taylor polynomial of e^r to degree 7 (truncation error
-//          r^8/8! < 6e-9 relative), scaled by 2^k through the exponent field.
-//   log  : x = m 2^e with m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s), s = (m-1)/(m+1),
-//          atanh series to s^11 (|s| <= 0.1716, truncation < 2e-9 relative).
-//   sin/cos : Cody & Waite reduction by pi/2 (two-part constant by FMA), quadrant select,
-//          Taylor polynomials of sin to r^9 and cos to r^10 on |r| <= pi/4.
+// Methods (table-driven reductions after Tang, ACM TOMS 15 (1989) and 16 (1990); no fitted
+// coefficients, every polynomial is a truncated Taylor series):
+//   exp  : x = (64 n + j) ln2/64 + r with a two-part ln2/64 applied by FMA, |r| <= ln2/128;
+//          e^x = 2^n 2^(j/64) (1 + p(r)), 2^(j/64) from a 64-entry table (high + low part),
+//          p the Taylor series of e^r - 1 to degree 4 (truncation < 4e-14).
+//   log  : x = 2^e m with m in [0.75, 1.5); nearest node c_i = 1 + i/128 (97-entry table of
+//          RN(1/c_i) and -log RN(1/c_i)); t = m RN(1/c_i) - 1 by one FMA, |t| < 0.0053;
+//          log x = e ln2 - log RN(1/c_i) + log1p(t), log1p by Taylor to degree 4.
+//   sin/cos : x = j 2pi/256 + r (two-part constant by FMA), |r| <= pi/256; angle addition with
+//          (sin, cos)(2 pi j/256) from a 256-entry table (high + low parts) and Taylor
+//          polynomials of sin r (to r^5) and cos r - 1 (to r^4).
 // Accuracy is within a few ulp of the correctly rounded result over the ranges the renderer
-// uses (tests/test_fmath.py checks it against libm in double precision and on the GPU
-// against CUDA's own expf/logf/sinf/cosf).
+// uses (tests/test_fmath.py checks it against libm in double precision). The table-reading
+// functions take the table base as an argument so that hot kernels can pass copies staged in
+// shared memory; the plain forms read the global copies (both hold the same values).
 #pragma once
 #include <stdint.h>
 #include <math.h>
 #include <string.h>
+
+#include "fmath_tables.h"
 
 #if defined(__CUDACC__)
 #define GX_HD __host__ __device__ __forceinline__
@@ -96,40 +103,85 @@ GX_HD uint32_t f2u(float x) {
 
 constexpr float kLn2Hi = 0.693147182f;          // nearest f32 to ln 2
 constexpr float kLn2Lo = -1.904654300e-09f;     // ln 2 - kLn2Hi
-constexpr float kLog2e = 1.44269502f;
-constexpr float kPio2Hi = 1.57079637f;          // nearest f32 to pi/2
-constexpr float kPio2Lo = -4.37113900e-08f;     // pi/2 - kPio2Hi
-constexpr float kTwoOverPi = 0.636619747f;
 
 // 2^k as a float for k in [-126, 127].
 GX_HD float pow2i(int k) { return b2f((uint32_t)(k + 127) << 23); }
 
-GX_HD float exp(float x) {
+// Global table copies: the device arrays in device code, the host arrays in host code.
+GX_HD const float* tab_log() {
+#if defined(__CUDA_ARCH__)
+    return kLogTabD;
+#else
+    return kLogTabH;
+#endif
+}
+GX_HD const float* tab_exp() {
+#if defined(__CUDA_ARCH__)
+    return kExpTabD;
+#else
+    return kExpTabH;
+#endif
+}
+GX_HD const float* tab_sc() {
+#if defined(__CUDA_ARCH__)
+    return kScTabD;
+#else
+    return kScTabH;
+#endif
+}
+// two consecutive floats of a table (8-byte aligned pairs)
+GX_HD void ld2(const float* T, int k, float* a, float* b) {
+#if defined(__CUDA_ARCH__)
+    float2 v = *reinterpret_cast<const float2*>(T + 2 * k);
+    *a = v.x;
+    *b = v.y;
+#else
+    *a = T[2 * k];
+    *b = T[2 * k + 1];
+#endif
+}
+// one 16-byte table row
+GX_HD void ld4(const float* T, int k, float* a, float* b, float* c, float* d) {
+#if defined(__CUDA_ARCH__)
+    float4 v = *reinterpret_cast<const float4*>(T + 4 * k);
+    *a = v.x;
+    *b = v.y;
+    *c = v.z;
+    *d = v.w;
+#else
+    *a = T[4 * k];
+    *b = T[4 * k + 1];
+    *c = T[4 * k + 2];
+    *d = T[4 * k + 3];
+#endif
+}
+
+GX_HD float exp_t(float x, const float* T) {
     // one range test: NaN, overflow and the subnormal/underflow tail take the slow branch
     if (!(x >= -87.3365479f && x <= 88.7228394f)) {
         if (x != x) return x;
         if (x > 88.7228394f) return b2f(0x7F800000u);
         if (x < -103.972084f) return 0.0f;
     }
-    float kf = rint_(x * kLog2e);
-    float r = fma_(kf, -kLn2Hi, x);
-    r = fma_(kf, -kLn2Lo, r);
-    // Taylor series of e^r, Horner form, coefficients 1/n!.
-    float p = 1.98412698e-4f;                // 1/5040
-    p = fma_(p, r, 1.38888889e-3f);          // 1/720
-    p = fma_(p, r, 8.33333377e-3f);          // 1/120
-    p = fma_(p, r, 4.16666679e-2f);          // 1/24
-    p = fma_(p, r, 1.66666672e-1f);          // 1/6
-    p = fma_(p, r, 0.5f);
-    p = fma_(p, r, 1.0f);
-    p = fma_(p, r, 1.0f);
+    float kf = rint_(x * kExpK);
+    float r = fma_(kf, -kExpLHi, x);
+    r = fma_(kf, -kExpLLo, r);
     int k = (int)kf;
-    if (k >= -126 && k <= 127) return p * pow2i(k);
-    if (k > 127) return (p * 2.0f) * pow2i(k - 1);
-    return (p * pow2i(k + 64)) * pow2i(-64);
+    int n = k >> 6;  // k = 64 n + j
+    float th, tl;
+    ld2(T, k & 63, &th, &tl);
+    // e^r - 1 = r + r^2 (1/2 + r/6 + r^2/24)
+    float q = fma_(r, 4.16666679e-2f, 1.66666672e-1f);  // 1/24, 1/6
+    q = fma_(r, q, 0.5f);
+    float p = fma_(r * r, q, r);
+    float v = th + fma_(th, p, tl);
+    if (n >= -126 && n <= 127) return v * pow2i(n);
+    if (n > 127) return (v * 2.0f) * pow2i(n - 1);
+    return (v * pow2i(n + 64)) * pow2i(-64);
 }
+GX_HD float exp(float x) { return exp_t(x, tab_exp()); }
 
-GX_HD float log(float x) {
+GX_HD float log_t(float x, const float* T) {
     uint32_t b = f2b(x);
     int e = 0;
     if (b - 0x00800000u >= 0x7F000000u) {  // one test: zero, subnormal, negative, infinite or NaN
@@ -140,58 +192,38 @@ GX_HD float log(float x) {
         b = f2b(x);
         e = -23;
     }
-    e += (int)(b >> 23) - 127;
-    float m = b2f((b & 0x007FFFFFu) | 0x3F800000u);
-    if (m > 1.41421354f) {
-        m = m * 0.5f;
-        e += 1;
-    }
-    float f = m - 1.0f;
-    float s = div_(f, 2.0f + f);
-    float z = s * s;
-    // 2 atanh(s) = 2 s (1 + z/3 + z^2/5 + ... + z^5/11)
-    float p = 9.09090936e-2f;                // 1/11
-    p = fma_(p, z, 1.11111112e-1f);          // 1/9
-    p = fma_(p, z, 1.42857149e-1f);          // 1/7
-    p = fma_(p, z, 2.00000003e-1f);          // 1/5
-    p = fma_(p, z, 3.33333343e-1f);          // 1/3
-    p = fma_(p, z, 1.0f);
-    float lm = (2.0f * s) * p;
-    float ef = (float)e;
-    return fma_(ef, kLn2Hi, fma_(ef, kLn2Lo, lm));
+    const uint32_t mb = b & 0x007FFFFFu;
+    const uint32_t big = mb >= 0x00400000u ? 1u : 0u;  // mantissa >= 1.5: halve it
+    e += (int)(b >> 23) - 127 + (int)big;
+    const float m = b2f(mb | (big ? 0x3F000000u : 0x3F800000u));  // m in [0.75, 1.5)
+    const int i = (int)rint_((m - 1.0f) * 128.0f);               // nearest node, -32..64
+    float rinv, thi, tlo, pad;
+    ld4(T, i + 32, &rinv, &thi, &tlo, &pad);
+    const float t = fma_(m, rinv, -1.0f);
+    // log1p(t) = t + t^2 (-1/2 + t/3 - t^2/4)
+    float q = fma_(t, -0.25f, 3.33333343e-1f);
+    q = fma_(t, q, -0.5f);
+    const float p = fma_(t * t, q, t);
+    const float ef = (float)e;
+    return fma_(ef, kLn2Hi, thi) + (fma_(ef, kLn2Lo, tlo) + p);
 }
-
-GX_HD float sin_poly(float r) {
-    float z = r * r;
-    float p = 2.75573188e-6f;                // 1/9!
-    p = fma_(p, z, -1.98412701e-4f);         // -1/7!
-    p = fma_(p, z, 8.33333377e-3f);          // 1/5!
-    p = fma_(p, z, -1.66666672e-1f);         // -1/3!
-    return fma_(p * z, r, r);
-}
-GX_HD float cos_poly(float r) {
-    float z = r * r;
-    float p = -2.75573188e-7f;               // -1/10!
-    p = fma_(p, z, 2.48015876e-5f);          // 1/8!
-    p = fma_(p, z, -1.38888892e-3f);         // -1/6!
-    p = fma_(p, z, 4.16666679e-2f);          // 1/4!
-    p = fma_(p, z, -0.5f);
-    return fma_(p, z, 1.0f);
-}
+GX_HD float log(float x) { return log_t(x, tab_log()); }
 
 // sin and cos of x together; accurate for |x| < 1e4 (the renderer's angles are 2 pi U).
-GX_HD void sincos(float x, float* s, float* c) {
-    float kf = rint_(x * kTwoOverPi);
-    float r = fma_(kf, -kPio2Hi, x);
-    r = fma_(kf, -kPio2Lo, r);
-    float sp = sin_poly(r), cp = cos_poly(r);
-    // quadrant q: odd q swaps sin and cos; sin is negated for q = 2, 3 and cos for q = 1, 2
-    uint32_t q = (uint32_t)(int)kf;
-    float so = (q & 1u) ? cp : sp;
-    float co = (q & 1u) ? sp : cp;
-    *s = b2f(f2b(so) ^ ((q & 2u) << 30));
-    *c = b2f(f2b(co) ^ (((q + 1u) & 2u) << 30));
+GX_HD void sincos_t(float x, const float* T, float* s, float* c) {
+    float kf = rint_(x * kScK);
+    float r = fma_(kf, -kScPHi, x);
+    r = fma_(kf, -kScPLo, r);
+    float sh, ch, sl, cl;
+    ld4(T, (int)kf & 255, &sh, &ch, &sl, &cl);
+    float z = r * r;
+    float sr = fma_(z * r, fma_(z, 8.33333377e-3f, -1.66666672e-1f), r);  // sin r: 1/120, -1/6
+    float cm = z * fma_(z, 4.16666679e-2f, -0.5f);                        // cos r - 1: 1/24, -1/2
+    // sin(a + r) = sin a + (sin a (cos r - 1) + cos a sin r), the table's residual folded in
+    *s = sh + fma_(ch, sr, fma_(sh, cm, sl));
+    *c = ch + fma_(-sh, sr, fma_(ch, cm, cl));
 }
+GX_HD void sincos(float x, float* s, float* c) { sincos_t(x, tab_sc(), s, c); }
 GX_HD float sin(float x) { float s, c; sincos(x, &s, &c); return s; }
 GX_HD float cos(float x) { float s, c; sincos(x, &s, &c); return c; }
 

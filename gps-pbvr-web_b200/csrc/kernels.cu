@@ -349,13 +349,14 @@ __device__ __forceinline__ void splat_write(ull* sub, uint32_t idx, float depth_
 }
 
 // emit_particle (gps_splat.wgsl:259-282) with the packed winner rule
-__device__ __forceinline__ uint32_t emit_gps(const FrameConst& f, const float* lut, uint32_t i, uint32_t& rs, float4 r0,
-                                             float4 r1, float4 r2, ull* sub) {
+__device__ __forceinline__ uint32_t emit_gps(const FrameConst& f, const FTabs& T, const float* lut, uint32_t i, uint32_t& rs,
+                                             float4 r0, float4 r1, float4 r2, ull* sub) {
     float u = gx::next_u(&rs);
-    float r = f.exact_radius ? corrected_radius_exact(r0.w, r2.y, u) : corrected_radius_lut(lut, __float_as_uint(r2.x), r1.w, u);
+    float r = f.exact_radius ? corrected_radius_exact(r0.w, r2.y, u)
+                             : corrected_radius_lut(lut, __float_as_uint(r2.x), r1.w, u, T.lg);
     float th = gxc::kTwoPi * gx::next_u(&rs);
     float sn, cs;
-    gx::sincos(th, &sn, &cs);
+    gx::sincos_t(th, T.sc, &sn, &cs);
     float wx = r * cs, wy = r * sn;
     float px_ = r0.x + r1.x * wx;
     float py_ = r0.y + (r1.y * wx + r1.z * wy);
@@ -369,15 +370,16 @@ __device__ __forceinline__ uint32_t emit_gps(const FrameConst& f, const float* l
 
 struct Normal {
     uint32_t* st;
+    const FTabs& T;
     bool has;
     float spare;
     __device__ __forceinline__ float next() {
         if (has) { has = false; return spare; }
         float u1 = fmax_(gx::next_u(st), gxc::kUMin);
         float u2 = gx::next_u(st);
-        float r = sqrt_(-F_(2.0) * gx::log(u1));
+        float r = sqrt_(-F_(2.0) * gx::log_t(u1, T.lg));
         float sn, cs;
-        gx::sincos(gxc::kTwoPi * u2, &sn, &cs);
+        gx::sincos_t(gxc::kTwoPi * u2, T.sc, &sn, &cs);
         spare = r * sn;
         has = true;
         return r * cs;
@@ -385,8 +387,9 @@ struct Normal {
 };
 
 // emit_particle_pbvr (gps_splat.wgsl:490-532); returns bit 0 = counts as a point, bit 1 = written
-__device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, uint32_t i, uint32_t& rs, const float4* R, ull* sub) {
-    Normal nm{&rs, false, F_(0.0)};
+__device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, const FTabs& T, uint32_t i, uint32_t& rs, const float4* R,
+                                              ull* sub) {
+    Normal nm{&rs, T, false, F_(0.0)};
     float uz = nm.next();
     float uy = nm.next();
     float ux = nm.next();
@@ -419,8 +422,8 @@ __device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, uint32_t i, u
         float r2v = r2.w * dvx * dvx + F_(2.0) * r3.x * dvx * dvy + r3.y * dvy * dvy;
         // radial_keep (gps_splat.wgsl:434-438) with h(min(o, 1-1e-6)) hoisted per splat
         float oo = fmin_(r0.w, gxc::kOneMinus1e6);
-        float y = oo * gx::exp(-F_(0.5) * fmax_(r2v, F_(0.0)));
-        float keep = clamp_(div_(eol(y), r1.y), F_(0.0), F_(1.0));
+        float y = oo * gx::exp_t(-F_(0.5) * fmax_(r2v, F_(0.0)), T.ex);
+        float keep = clamp_(div_(eol(y, T.lg), r1.y), F_(0.0), F_(1.0));
         if (gx::next_u(&rs) >= keep) return 0u;
     }
     float depth_z = (flags & FLAG_CENTRE) ? r0.z : cz;
@@ -433,8 +436,8 @@ __device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, uint32_t i, u
 }
 
 // ScreenOccupancy branch of particle_pass (gps_splat.wgsl:686-708); returns 1 on a hit
-__device__ __forceinline__ uint32_t emit_so(const FrameConst& f, uint32_t i, uint32_t k, uint32_t& rs, const float4* R,
-                                            ull* sub) {
+__device__ __forceinline__ uint32_t emit_so(const FrameConst& f, const FTabs& T, uint32_t i, uint32_t k, uint32_t& rs,
+                                            const float4* R, ull* sub) {
     float4 r0 = R[0], b = R[1];
     const uint32_t side = f.side, samples = f.S;
     bool sparse = R[3].w > F_(0.0);
@@ -450,17 +453,16 @@ __device__ __forceinline__ uint32_t emit_so(const FrameConst& f, uint32_t i, uin
     float dx = (float)xx + uvx - r0.x, dy = (float)yy + uvy - r0.y;
     float4 inv = R[2];
     float r2 = fmax_(inv.x * dx * dx + F_(2.0) * inv.y * dx * dy + inv.z * dy * dy, F_(0.0));
-    float alpha = fmin_(r0.w * gx::exp(-F_(0.5) * r2), gxc::kOneMinus1e6);
+    float alpha = fmin_(r0.w * gx::exp_t(-F_(0.5) * r2, T.ex), gxc::kOneMinus1e6);
     float coverage;
-    if (sparse) coverage = div_(-gx::log(F_(1.0) - alpha), inv.w);
-    else coverage = F_(1.0) - gx::exp(f.density * gx::log(F_(1.0) - alpha));
+    if (sparse) coverage = div_(-gx::log_t(F_(1.0) - alpha, T.lg), inv.w);
+    else coverage = F_(1.0) - gx::exp_t(f.density * gx::log_t(F_(1.0) - alpha, T.lg), T.ex);
     if (gx::next_u(&rs) >= coverage) return 0u;
     splat_write(sub, (yy * f.W + xx) * samples + sub_i, r0.z, i);
     return 1u;
 }
 
 constexpr int kPT = 256;               // threads per particle block
-constexpr int kMaxE = 1024;            // ensembles per batch (shared prefix table)
 
 // Largest j in [lo, hi) with off(j) <= v, by a 32-ary warp search (off(lo) <= v must hold).
 __device__ __forceinline__ uint32_t warp_last_le(const uint2* __restrict__ L, uint32_t lo, uint32_t hi, uint64_t v, int lane) {
@@ -489,12 +491,14 @@ __global__ void __launch_bounds__(kPT, GPSB_PARTICLE_MIN_BLOCKS) k_particles(Fra
                                                    const EnsTotal* __restrict__ etot, uint32_t first_seed, uint32_t E,
                                                    ull* sub, uint32_t* unit_counter, ull* stats) {
     constexpr int kPTile = kPT * kPIPT;  // particles per tile
-    // dynamic shared memory: [entry offsets (kPTile + 2)] [entry ids (kPTile + 2)] [radius table (GPS)]
-    extern __shared__ uint32_t s_dyn[];
-    uint32_t* s_off = s_dyn;
-    uint32_t* s_id = s_dyn + (kPTile + 2);
-    float* s_lut = reinterpret_cast<float*>(s_dyn + 2 * (kPTile + 2));
-    __shared__ uint64_t s_ubase[kMaxE + 1];
+    // dynamic shared memory: [fmath tables (kTabFloats)] [first unit of each ensemble (E + 1)]
+    // [entry offsets (kPTile + 2)] [entry ids (kPTile + 2)] [radius table (GPS)]
+    extern __shared__ __align__(16) uint32_t s_dyn[];
+    const FTabs T = stage_tabs(reinterpret_cast<float*>(s_dyn));
+    uint64_t* s_ubase = reinterpret_cast<uint64_t*>(s_dyn + kTabFloats);
+    uint32_t* s_off = s_dyn + kTabFloats + 2 * (E + 1);
+    uint32_t* s_id = s_off + (kPTile + 2);
+    float* s_lut = reinterpret_cast<float*>(s_id + (kPTile + 2));
     __shared__ uint32_t s_unit, s_j0, s_w;
     const int tid = threadIdx.x, lane = tid & 31;
     const bool use_lut = MC == 0 && !f.exact_radius;
@@ -582,13 +586,13 @@ __global__ void __launch_bounds__(kPT, GPSB_PARTICLE_MIN_BLOCKS) k_particles(Fra
                 }
                 uint32_t rs = gx::particle_seed(i, k + 1u, seed);
                 if (MC == 0) {
-                    writes += emit_gps(f, s_lut, i, rs, R[0], R[1], R[2], S);
+                    writes += emit_gps(f, T, s_lut, i, rs, R[0], R[1], R[2], S);
                 } else if (MC == 1) {
-                    uint32_t r = emit_pbvr(f, i, rs, R, S);
+                    uint32_t r = emit_pbvr(f, T, i, rs, R, S);
                     points += r & 1u;
                     writes += r >> 1;
                 } else {
-                    uint32_t r = emit_so(f, i, k, rs, R, S);
+                    uint32_t r = emit_so(f, T, i, k, rs, R, S);
                     points += r;
                     writes += r;
                 }
@@ -609,7 +613,7 @@ template <int MC, int IPT>
 static void launch_particles_t(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
                                const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
                                uint32_t* unit_counter, unsigned long long* stats, int grid, cudaStream_t st) {
-    size_t smem = 2 * (kPT * IPT + 2) * sizeof(uint32_t);
+    size_t smem = (kTabFloats + 2 * ((size_t)E + 1) + 2 * (kPT * IPT + 2)) * sizeof(uint32_t);
     if (MC == 0 && !fc.exact_radius) smem += kLutN * sizeof(float);
     static size_t attr = 0;
     if (smem > 48 * 1024 && smem > attr) {
@@ -668,7 +672,8 @@ __global__ void __launch_bounds__(128) k_primitive(FrameConst f, const float4* _
     float4 r0 = Rg[0], r1 = Rg[1], r2 = Rg[2];
     ull* S = sub + (size_t)e * ((uint64_t)f.W * f.H * f.S);
     ull writes = 0;
-    for (uint32_t q = 0; q < n; ++q) writes += emit_gps(f, lut, i, rs, r0, r1, r2, S);
+    const FTabs T{gx::tab_log(), gx::tab_exp(), gx::tab_sc()};
+    for (uint32_t q = 0; q < n; ++q) writes += emit_gps(f, T, lut, i, rs, r0, r1, r2, S);
     if (writes) atomicAdd(&stats[ST_WRITES], writes);
 }
 

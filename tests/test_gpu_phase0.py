@@ -89,9 +89,8 @@ def test_scan_sizes(n):
                                            (4_000_001, 0, False), (600_000, 0, True), (1_000_003, 1, False),
                                            (1_000_003, 2, True)])
 def test_scan_large_paths(n, offset, full):
-    """Sizes that take the persistent bulk-copy scan (16-byte aligned, n >= 2^19) with ragged
-    tails, full-range u32 counts whose total passes 2^32, and misaligned views that take the
-    per-tile kernel instead."""
+    """Many-tile scans with ragged tails, full-range u32 counts whose total passes 2^32, and
+    views that are not 16-byte aligned (scalar loads and stores instead of 128-bit ones)."""
     import torch
     dev = torch.device("cuda", 0)
     h = _pcg(np.arange(n, dtype=np.uint32) + np.uint32(offset * 77))
