@@ -22,6 +22,8 @@ CU_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler
                    "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-I" + os.path.join(CUDA, "include"),
              "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
+# extra nvcc flags for tuning builds (e.g. GPSB_NVCC_EXTRA="-DGPSB_SORT_LOOKAHEAD=16"; rebuild with --force)
+CU_FLAGS += os.environ.get("GPSB_NVCC_EXTRA", "").split()
 LIB_SOURCES = ["kernels.cu", "sorted.cu", "primitives.cu", "renderer.cpp", "hostmath.cpp", "ply.cpp"]
 
 

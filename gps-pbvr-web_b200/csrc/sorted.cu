@@ -47,6 +47,10 @@ constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRsIpt = 15;  // keys per thread: 3840 per tile, 30 KB of shared staging
 constexpr int kRsTile = kRsThreads * kRsIpt;
 constexpr int kMaxPasses = 8;
+#ifndef GPSB_SORT_LOOKAHEAD
+#define GPSB_SORT_LOOKAHEAD 8
+#endif
+constexpr int kRsLook = GPSB_SORT_LOOKAHEAD;  // predecessor tiles read per lookback round trip
 constexpr uint32_t kStAgg = 1u << 30, kStPre = 2u << 30, kStMask = (1u << 30) - 1u;
 
 template <int BITS>
@@ -80,7 +84,7 @@ __global__ void k_radix_hist_scan(uint32_t* hist, int passes) {
 }
 
 template <int BITS>
-__global__ void __launch_bounds__(kRsThreads) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+__global__ void __launch_bounds__(kRsThreads, 3) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                          uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                          uint32_t n, int shift, const uint32_t* __restrict__ gstart,
                                                          uint32_t* lookback, uint32_t* tile_counter, uint32_t* err) {
@@ -100,7 +104,7 @@ __global__ void __launch_bounds__(kRsThreads) k_onesweep(const uint32_t* __restr
     const uint32_t tile0 = t * kRsTile;
     const uint32_t tile_n = n - tile0 < (uint32_t)kRsTile ? n - tile0 : (uint32_t)kRsTile;
     const uint32_t base = tile0 + warp * 32 * kRsIpt;
-    uint32_t key[kRsIpt], val[kRsIpt], rank[kRsIpt];
+    uint32_t key[kRsIpt], rank[kRsIpt];
     const uint32_t lt = lanemask_lt();
     // rank every key within its warp's sub-tile in input order (stable): warp-match on the digit
 #pragma unroll
@@ -108,7 +112,6 @@ __global__ void __launch_bounds__(kRsThreads) k_onesweep(const uint32_t* __restr
         uint32_t idx = base + q * 32 + lane;
         bool valid = idx < n;
         key[q] = valid ? __ldg(&kin[idx]) : 0u;
-        val[q] = valid ? __ldg(&vin[idx]) : 0u;
         uint32_t d = valid ? ((key[q] >> shift) & (BINS - 1)) : (uint32_t)BINS;
         uint32_t peers = __match_any_sync(0xffffffffu, d);
         uint32_t before = valid ? s_wcnt[warp][d] : 0u;
@@ -142,7 +145,8 @@ __global__ void __launch_bounds__(kRsThreads) k_onesweep(const uint32_t* __restr
     for (int w = 0; w < warp; ++w) wbase += s_wsum[w];
     if (tid < BINS) s_dstart[tid] = wbase + incl - cnt;
     __syncthreads();
-    // scatter into shared memory in digit order (stable), then resolve the global offsets
+    // scatter into shared memory in digit order (stable); the values are read here, not held in
+    // registers through the ranking
 #pragma unroll
     for (int q = 0; q < kRsIpt; ++q) {
         uint32_t idx = base + q * 32 + lane;
@@ -150,25 +154,36 @@ __global__ void __launch_bounds__(kRsThreads) k_onesweep(const uint32_t* __restr
             uint32_t d = (key[q] >> shift) & (BINS - 1);
             uint32_t pos = s_dstart[d] + s_wcnt[warp][d] + rank[q];
             s_key[pos] = key[q];
-            s_val[pos] = val[q];
+            s_val[pos] = __ldg(&vin[idx]);
         }
     }
+    // lookback per digit, kRsLook predecessors per round trip; an unpublished word is polled again
     if (tid < BINS) {
         uint32_t excl = 0;
         if (t > 0) {
             int32_t pred = (int32_t)t - 1;
             uint32_t spins = 0;
             bool failed = false;
-            while (pred >= 0) {
-                uint32_t w = ld_relaxed32(&lookback[(size_t)pred * BINS + tid]);
-                if ((w >> 30) == 0u) {
+            while (true) {
+                uint32_t w[kRsLook];
+#pragma unroll
+                for (int u = 0; u < kRsLook; ++u)
+                    w[u] = pred - u >= 0 ? ld_relaxed32(&lookback[(size_t)(pred - u) * BINS + tid]) : kStPre;
+                int used = 0;
+                bool done = false;
+#pragma unroll
+                for (int u = 0; u < kRsLook; ++u) {
+                    if (done || used < u || (w[u] >> 30) == 0u) continue;
+                    excl += w[u] & kStMask;
+                    used = u + 1;
+                    done = (w[u] >> 30) == 2u;
+                }
+                if (done) break;
+                pred -= used;
+                if (used < kRsLook) {
                     if (++spins > (1u << 22)) { failed = true; break; }
                     __nanosleep(32);
-                    continue;
                 }
-                excl += w & kStMask;
-                if ((w >> 30) == 2u) break;
-                --pred;
             }
             if (failed) atomicOr(err, ERR_SORT_LOOKBACK);
             st_relaxed32(&lb[tid], kStPre | ((excl + cnt) & kStMask));
@@ -233,6 +248,8 @@ static cudaError_t radix_impl(RadixScratch& s, uint32_t* ka, uint32_t* va, uint3
         cudaMemcpyAsync(kb, ka, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
         cudaMemcpyAsync(vb, va, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
     }
+    // three resident blocks per SM need the largest shared-memory carveout (about 40 KB each)
+    cudaFuncSetAttribute(k_onesweep<BITS>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     for (int p = 0; p < passes; ++p) {
         k_onesweep<BITS><<<tiles, kRsThreads, 0, st>>>(ik, iv, ok, ov, n, p * BITS, hist + p * BINS,
                                                        (uint32_t*)s.lookback + (size_t)p * tiles * BINS,
