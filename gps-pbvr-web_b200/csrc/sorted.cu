@@ -44,13 +44,19 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // ============================================================================ radix sort
 constexpr int kRsThreads = 256;
 constexpr int kRsWarps = kRsThreads / 32;
-constexpr int kRsIpt = 15;  // keys per thread: 3840 per tile, 30 KB of shared staging
+constexpr int kRsIpt = 15;  // keys per thread: 3840 per tile, 37.5 KB of shared staging
 constexpr int kRsTile = kRsThreads * kRsIpt;
 constexpr int kMaxPasses = 8;
 #ifndef GPSB_SORT_LOOKAHEAD
 #define GPSB_SORT_LOOKAHEAD 8
 #endif
 constexpr int kRsLook = GPSB_SORT_LOOKAHEAD;  // predecessor tiles read per lookback round trip
+#ifndef GPSB_SORT_BALLOT_PEERS
+#define GPSB_SORT_BALLOT_PEERS 1
+#endif
+#ifndef GPSB_SORT_MIN_BLOCKS
+#define GPSB_SORT_MIN_BLOCKS 4
+#endif
 constexpr uint32_t kStAgg = 1u << 30, kStPre = 2u << 30, kStMask = (1u << 30) - 1u;
 
 template <int BITS>
@@ -84,7 +90,7 @@ __global__ void k_radix_hist_scan(uint32_t* hist, int passes) {
 }
 
 template <int BITS>
-__global__ void __launch_bounds__(kRsThreads, 3) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+__global__ void __launch_bounds__(kRsThreads, GPSB_SORT_MIN_BLOCKS) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                          uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                          uint32_t n, int shift, const uint32_t* __restrict__ gstart,
                                                          uint32_t* lookback, uint32_t* tile_counter, uint32_t* err) {
@@ -92,8 +98,9 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_onesweep(const uint32_t* __re
     __shared__ uint32_t s_wcnt[kRsWarps][BINS];  // per-warp digit counts, then exclusive prefix over warps
     __shared__ uint32_t s_dstart[BINS];          // tile-local exclusive prefix over digits
     __shared__ uint32_t s_gbase[BINS];           // global position of the digit's first key of this tile, minus s_dstart
-    __shared__ uint32_t s_key[kRsTile];
-    __shared__ uint32_t s_val[kRsTile];
+    __shared__ uint32_t s_key[kRsTile];                // keys in digit order
+    __shared__ uint16_t s_src[kRsTile];                // tile-local input index of each ordered key
+    __shared__ __align__(16) uint32_t s_vin[kRsTile];  // the tile's values in input order
     __shared__ uint32_t s_wsum[kRsWarps];
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -104,21 +111,50 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_onesweep(const uint32_t* __re
     const uint32_t tile0 = t * kRsTile;
     const uint32_t tile_n = n - tile0 < (uint32_t)kRsTile ? n - tile0 : (uint32_t)kRsTile;
     const uint32_t base = tile0 + warp * 32 * kRsIpt;
+    // the tile's values travel to shared memory asynchronously while the keys are ranked
+    const bool vasync = (((uintptr_t)vin) & 15u) == 0;
+    if (!vasync) {
+        for (uint32_t e = tid; e < tile_n; e += kRsThreads) s_vin[e] = vin[tile0 + e];
+    } else {
+        for (uint32_t c = tid; c < (uint32_t)kRsTile / 4u; c += kRsThreads) {
+            const uint32_t e = c * 4u;
+            const uint32_t bytes = e < tile_n ? min(tile_n - e, 4u) * 4u : 0u;
+            const uint32_t* src = bytes ? vin + tile0 + e : vin;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                             (uint32_t)__cvta_generic_to_shared(s_vin + e)),
+                         "l"(src), "r"(bytes)
+                         : "memory");
+        }
+    }
     uint32_t key[kRsIpt], rank[kRsIpt];
     const uint32_t lt = lanemask_lt();
-    // rank every key within its warp's sub-tile in input order (stable): warp-match on the digit
+    // rank every key within its warp's sub-tile in input order (stable): the lanes holding one digit
+    // find each other (peers: one ballot per digit bit, or match.any), the lowest of them adds the
+    // group's size to the warp's running count of that digit with a shared-memory atomic and
+    // passes the old count to its peers
 #pragma unroll
     for (int q = 0; q < kRsIpt; ++q) {
         uint32_t idx = base + q * 32 + lane;
         bool valid = idx < n;
         key[q] = valid ? __ldg(&kin[idx]) : 0u;
         uint32_t d = valid ? ((key[q] >> shift) & (BINS - 1)) : (uint32_t)BINS;
+#if GPSB_SORT_BALLOT_PEERS
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int b = 0; b < BITS; ++b) {
+            uint32_t m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? m : ~m;
+        }
+        if (!valid) peers = 0u;
+#else
         uint32_t peers = __match_any_sync(0xffffffffu, d);
-        uint32_t before = valid ? s_wcnt[warp][d] : 0u;
-        rank[q] = before + __popc(peers & lt);
-        __syncwarp();
-        if (valid && (peers & lt) == 0u) s_wcnt[warp][d] = before + __popc(peers);
-        __syncwarp();
+#endif
+        int leader = peers ? __ffs(peers) - 1 : lane;
+        uint32_t old = 0u;
+        if (valid && leader == lane) old = atomicAdd(&s_wcnt[warp][d], (uint32_t)__popc(peers));
+        old = __shfl_sync(0xffffffffu, old, leader);
+        rank[q] = old + __popc(peers & lt);
+        __syncwarp();  // orders this key's count update before the next key's (other leader lanes)
     }
     __syncthreads();
     // per digit: exclusive prefix over warps and the tile count; publish the tile's aggregate early
@@ -144,9 +180,9 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_onesweep(const uint32_t* __re
     uint32_t wbase = 0;
     for (int w = 0; w < warp; ++w) wbase += s_wsum[w];
     if (tid < BINS) s_dstart[tid] = wbase + incl - cnt;
+    if (vasync) asm volatile("cp.async.wait_all;" ::: "memory");  // own copies done; the barrier shares them
     __syncthreads();
-    // scatter into shared memory in digit order (stable); the values are read here, not held in
-    // registers through the ranking
+    // scatter into shared memory in digit order (stable); values follow through their input index
 #pragma unroll
     for (int q = 0; q < kRsIpt; ++q) {
         uint32_t idx = base + q * 32 + lane;
@@ -154,7 +190,7 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_onesweep(const uint32_t* __re
             uint32_t d = (key[q] >> shift) & (BINS - 1);
             uint32_t pos = s_dstart[d] + s_wcnt[warp][d] + rank[q];
             s_key[pos] = key[q];
-            s_val[pos] = __ldg(&vin[idx]);
+            s_src[pos] = (uint16_t)(idx - tile0);
         }
     }
     // lookback per digit, kRsLook predecessors per round trip; an unpublished word is polled again
@@ -197,7 +233,7 @@ __global__ void __launch_bounds__(kRsThreads, 3) k_onesweep(const uint32_t* __re
         uint32_t pos = s_gbase[(k >> shift) & (BINS - 1)] + i;
         if (pos < n) {
             kout[pos] = k;
-            vout[pos] = s_val[i];
+            vout[pos] = s_vin[s_src[i]];
         } else {
             atomicOr(err, ERR_BAD_INDEX);
         }
@@ -248,7 +284,7 @@ static cudaError_t radix_impl(RadixScratch& s, uint32_t* ka, uint32_t* va, uint3
         cudaMemcpyAsync(kb, ka, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
         cudaMemcpyAsync(vb, va, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
     }
-    // three resident blocks per SM need the largest shared-memory carveout (about 40 KB each)
+    // four resident blocks per SM need the largest shared-memory carveout (48 KB each)
     cudaFuncSetAttribute(k_onesweep<BITS>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     for (int p = 0; p < passes; ++p) {
         k_onesweep<BITS><<<tiles, kRsThreads, 0, st>>>(ik, iv, ok, ov, n, p * BITS, hist + p * BINS,
