@@ -112,6 +112,10 @@ SIGNATURES = {
     "gpsb_sort_pairs": (ST, [P, P, P, P, P, U32, U32]),
     "gpsb_p0_sample": (ST, [P, U32, U32, U32, U32, P]),
     "gpsb_get_tuning": (ST, [P, P]),
+    # denoiser kernels (return cudaError_t codes)
+    "gpsb_dn_conv_fwd": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, ST, P, P, ST, ST, ST, ST, P, P]),
+    "gpsb_dn_conv_dw": (ST, [P, ST, P, ST, ST, ST, ST, ST, ST, ST, ST, P, P, P]),
+    "gpsb_dn_flip": (ST, [P, ST, ST, ST, P, ST, ST, P]),
 }
 
 _lib = None
