@@ -74,6 +74,7 @@ SIGNATURES = {
     "gpsb_create": (ST, [C.c_int, U32, U32, U32, P]),
     "gpsb_destroy": (None, [P]),
     "gpsb_set_stream": (ST, [P, P]),
+    "gpsb_set_feature_accum": (ST, [P, P]),
     "gpsb_set_gaussians": (ST, [P, P, SZ]),
     "gpsb_set_gaussians_sh": (ST, [P, P, SZ, P, SZ, U32]),
     "gpsb_set_gaussians_sh_device": (ST, [P, P, SZ, P, SZ, U32]),
@@ -116,6 +117,18 @@ SIGNATURES = {
     "gpsb_dn_conv_fwd": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, ST, P, P, ST, ST, ST, ST, P, P]),
     "gpsb_dn_conv_dw": (ST, [P, ST, P, ST, ST, ST, ST, ST, ST, ST, ST, P, P, P]),
     "gpsb_dn_flip": (ST, [P, ST, ST, ST, P, ST, ST, P]),
+    "gpsb_dn_relu_bwd": (ST, [P, ST, ST, P, ST, ST, ST, ST, P, ST, P]),
+    "gpsb_dn_up2": (ST, [P, ST, ST, ST, ST, ST, P, ST, ST, P]),
+    "gpsb_dn_up2_bwd": (ST, [P, ST, ST, ST, ST, ST, ST, P, P]),
+    "gpsb_dn_pool2": (ST, [P, ST, ST, ST, ST, ST, ST, P, P]),
+    "gpsb_dn_pool2_bwd_add": (ST, [P, ST, ST, ST, ST, P, ST, ST, P]),
+    "gpsb_dn_bias_grad": (ST, [P, ST, ST, ST, P, P]),
+    "gpsb_dn_l1": (ST, [P, P, P, ST, P, P, C.c_float, P]),
+    "gpsb_dn_residual": (ST, [P, P, ST, P, P]),
+    "gpsb_dn_adam": (ST, [P, P, P, P, ST, C.c_float, C.c_float, C.c_float, C.c_float, ST, P, P]),
+    "gpsb_dn_to_bf16": (ST, [P, ST, ST, ST, P, ST, P]),
+    "gpsb_dn_pack": (ST, [P, P, ST, P, P, P]),
+    "gpsb_dn_crop": (ST, [P, P, P, ST, ST, P, ST, ST, ST, P, P, P, P]),
 }
 
 _lib = None

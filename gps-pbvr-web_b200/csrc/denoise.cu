@@ -191,6 +191,166 @@ __global__ void k_flip(const bf16* w, int cout, int cin, int kp, bf16* wf, int c
     wf[i] = v;
 }
 
+
+// ---------------------------------------------------------------------------- element-wise steps
+__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+
+// out[m][c] = g[m][goff + c] * (y[m][yoff + c] > 0) for c < C (y null: no mask), 0 for C <= c < ldo
+__global__ void k_relu_bwd(const float* g, int ldg, int goff, const bf16* y, int ldy, int yoff, int M, int C, bf16* out,
+                           int ldo) {
+    const int i = gtid();
+    if (i >= M * ldo) return;
+    const int m = i / ldo, c = i - m * ldo;
+    float v = 0.0f;
+    if (c < C) {
+        v = g[(size_t)m * ldg + goff + c];
+        if (y && !(__bfloat162float(y[(size_t)m * ldy + yoff + c]) > 0.0f)) v = 0.0f;
+    }
+    out[i] = __float2bfloat16_rn(v);
+}
+
+// nearest 2x upsampling of src (B, h, w, lds) channels [0, C) into dst (B, 2h, 2w, ldd) at doff
+__global__ void k_up2(const bf16* src, int lds, int B, int h, int w, int C, bf16* dst, int ldd, int doff) {
+    const int i = gtid();
+    const int H = 2 * h, W = 2 * w;
+    if (i >= B * H * W * C) return;
+    const int c = i % C, px = i / C, X = px % W, Y = (px / W) % H, b = px / (W * H);
+    dst[(size_t)px * ldd + doff + c] = src[((size_t)(b * h + Y / 2) * w + X / 2) * lds + c];
+}
+// out (B, h, w, C) = sum over each 2x2 block of g (B, 2h, 2w, ldg) channels [goff, goff + C)
+__global__ void k_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int C, float* out) {
+    const int i = gtid();
+    if (i >= B * h * w * C) return;
+    const int c = i % C, px = i / C, x = px % w, y = (px / w) % h, b = px / (w * h);
+    const int W = 2 * w;
+    float s = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) s += g[((size_t)(b * 2 * h + 2 * y + (d >> 1)) * W + 2 * x + (d & 1)) * ldg + goff + c];
+    out[i] = s;
+}
+// 2x2 average pooling of src (B, 2h, 2w, lds) channels [soff, soff + C) into dst (B, h, w, C)
+__global__ void k_pool2(const bf16* src, int lds, int soff, int B, int h, int w, int C, bf16* dst) {
+    const int i = gtid();
+    if (i >= B * h * w * C) return;
+    const int c = i % C, px = i / C, x = px % w, y = (px / w) % h, b = px / (w * h);
+    const int W = 2 * w;
+    float s = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 4; ++d)
+        s += __bfloat162float(src[((size_t)(b * 2 * h + 2 * y + (d >> 1)) * W + 2 * x + (d & 1)) * lds + soff + c]);
+    dst[i] = __float2bfloat16_rn(0.25f * s);
+}
+// acc (B, 2h, 2w, lda) channels [aoff, aoff + C) += g (B, h, w, C) / 4 spread over each 2x2 block
+__global__ void k_pool2_bwd_add(const float* g, int B, int h, int w, int C, float* acc, int lda, int aoff) {
+    const int i = gtid();
+    const int H = 2 * h, W = 2 * w;
+    if (i >= B * H * W * C) return;
+    const int c = i % C, px = i / C, X = px % W, Y = (px / W) % H, b = px / (W * H);
+    acc[(size_t)px * lda + aoff + c] += 0.25f * g[((size_t)(b * h + Y / 2) * w + X / 2) * C + c];
+}
+// db[c] += sum_m dz[m][c]: one block per 256-pixel chunk, shared partial sums, one atomic per channel
+__global__ void k_bias_grad(const bf16* dz, int ld, int M, int C, float* db) {
+    __shared__ float s[256];
+    for (int c = threadIdx.x; c < C; c += blockDim.x) s[c] = 0.0f;
+    __syncthreads();
+    const int m0 = blockIdx.x * 256;
+    for (int i = threadIdx.x; i < 256 * C; i += blockDim.x) {
+        const int m = m0 + i / C, c = i % C;
+        if (m < M) atomicAdd(&s[c], __bfloat162float(dz[(size_t)m * ld + c]));
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&db[c], s[c]);
+}
+// L1 loss of pred = base + r against target (M x 3, fp32): loss_sum += sum |d|, dr[m][0..7] = scale * sign(d)
+__global__ void k_l1(const float* base, const float* r, const float* target, int M, float* loss_sum, bf16* dr,
+                     float scale) {
+    const int m = gtid();
+    float l = 0.0f;
+    if (m < M) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float gsgn = 0.0f;
+            if (c < 3) {
+                const float d = base[(size_t)m * 3 + c] + r[(size_t)m * 3 + c] - target[(size_t)m * 3 + c];
+                l += fabsf(d);
+                gsgn = d > 0.0f ? scale : (d < 0.0f ? -scale : 0.0f);
+            }
+            dr[(size_t)m * 8 + c] = __float2bfloat16_rn(gsgn);
+        }
+    }
+    for (int o = 16; o; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss_sum, l);
+}
+// out = base + r (M x 3)
+__global__ void k_residual(const float* base, const float* r, int n, float* out) {
+    const int i = gtid();
+    if (i < n) out[i] = base[i] + r[i];
+}
+// Adam (Kingma & Ba 2015) on fp32 master weights; wb (optional) receives the bf16 copy
+__global__ void k_adam(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
+                       float c1, float c2, bf16* wb) {
+    const int i = gtid();
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16_rn(wi);
+}
+// fp32 -> bf16 copy with a row length change: dst[r][c] = c < cols ? src[r * lds + c] : 0 (c < ldd)
+__global__ void k_to_bf16(const float* src, int lds, int rows, int cols, bf16* dst, int ldd) {
+    const int i = gtid();
+    if (i >= rows * ldd) return;
+    const int r = i / ldd, c = i - r * ldd;
+    dst[i] = __float2bfloat16_rn(c < cols ? src[(size_t)r * lds + c] : 0.0f);
+}
+
+// Denoiser input of one frame from the renderer's accumulation (rgb sum, count) and feature sums
+// (per pixel: sum r^2, g^2, b^2, alpha, depth * alpha): x (P x 8 bf16) = (mean rgb, d / (1 + d) of
+// the mean covered depth, mean alpha, per-pixel ensemble standard deviation, 0, 0); base (P x 3) =
+// mean rgb.
+__global__ void k_pack(const float4* accum, const float* feat, int P, bf16* x, float* base) {
+    const int p = gtid();
+    if (p >= P) return;
+    const float4 a = accum[p];
+    const float n = fmaxf(a.w, 1.0f);
+    const float mr = a.x / n, mg = a.y / n, mb = a.z / n;
+    float f[8] = {mr, mg, mb, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (feat) {
+        const float* q = feat + (size_t)p * 8;
+        const float va = fmaxf(q[0] / n - mr * mr, 0.0f) + fmaxf(q[1] / n - mg * mg, 0.0f) + fmaxf(q[2] / n - mb * mb, 0.0f);
+        const float alpha = q[3] / n;
+        const float depth = q[3] > 0.0f ? q[4] / q[3] : 0.0f;
+        f[3] = depth / (1.0f + depth);
+        f[4] = alpha;
+        f[5] = sqrtf(va / 3.0f);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x[(size_t)p * 8 + c] = __float2bfloat16_rn(f[c]);
+    base[(size_t)p * 3 + 0] = mr;
+    base[(size_t)p * 3 + 1] = mg;
+    base[(size_t)p * 3 + 2] = mb;
+}
+
+// Training batch: crop b takes the ch x cw window at (y0, x0) of image img from the stacked frames
+// (x: N x H x W x 8 bf16, base and target: N x H x W x 3 fp32); crops[b] = (img, y0, x0).
+__global__ void k_crop(const bf16* x, const float* base, const float* target, int H, int W, const int* crops, int B,
+                       int ch, int cw, bf16* xb, float* baseb, float* targetb) {
+    const int i = gtid();
+    if (i >= B * ch * cw) return;
+    const int b = i / (ch * cw), yx = i - b * ch * cw, y = yx / cw, xq = yx - y * cw;
+    const int img = crops[3 * b], y0 = crops[3 * b + 1], x0 = crops[3 * b + 2];
+    const size_t src = ((size_t)img * H + y0 + y) * W + x0 + xq;
+    *reinterpret_cast<uint4*>(xb + (size_t)i * 8) = *reinterpret_cast<const uint4*>(x + src * 8);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        baseb[(size_t)i * 3 + c] = base[src * 3 + c];
+        targetb[(size_t)i * 3 + c] = target[src * 3 + c];
+    }
+}
 }  // namespace dn
 }  // namespace gpsb
 
@@ -259,6 +419,68 @@ int gpsb_dn_flip(const void* w, int cout, int cin, int kp, void* wf, int coutp, 
     if (kp2 % 64 || kp2 < 9 * coutp || coutp < cout) return (int)cudaErrorInvalidValue;
     const int n = cin * kp2;
     k_flip<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const bf16*)w, cout, cin, kp, (bf16*)wf, coutp, kp2);
+    return (int)cudaGetLastError();
+}
+
+static inline int grid_of(long n) { return (int)((n + 255) / 256); }
+
+int gpsb_dn_relu_bwd(const float* g, int ldg, int goff, const void* y, int ldy, int yoff, int M, int C, void* out,
+                     int ldo, void* stream) {
+    if (C > ldo) return (int)cudaErrorInvalidValue;
+    k_relu_bwd<<<grid_of((long)M * ldo), 256, 0, (cudaStream_t)stream>>>(g, ldg, goff, (const bf16*)y, ldy, yoff, M, C,
+                                                                          (bf16*)out, ldo);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_up2(const void* src, int lds, int B, int h, int w, int C, void* dst, int ldd, int doff, void* stream) {
+    k_up2<<<grid_of(4L * B * h * w * C), 256, 0, (cudaStream_t)stream>>>((const bf16*)src, lds, B, h, w, C, (bf16*)dst,
+                                                                          ldd, doff);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int C, float* out, void* stream) {
+    k_up2_bwd<<<grid_of((long)B * h * w * C), 256, 0, (cudaStream_t)stream>>>(g, ldg, goff, B, h, w, C, out);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_pool2(const void* src, int lds, int soff, int B, int h, int w, int C, void* dst, void* stream) {
+    k_pool2<<<grid_of((long)B * h * w * C), 256, 0, (cudaStream_t)stream>>>((const bf16*)src, lds, soff, B, h, w, C,
+                                                                             (bf16*)dst);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_pool2_bwd_add(const float* g, int B, int h, int w, int C, float* acc, int lda, int aoff, void* stream) {
+    k_pool2_bwd_add<<<grid_of(4L * B * h * w * C), 256, 0, (cudaStream_t)stream>>>(g, B, h, w, C, acc, lda, aoff);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_bias_grad(const void* dz, int ld, int M, int C, float* db, void* stream) {
+    if (C > 256) return (int)cudaErrorInvalidValue;
+    k_bias_grad<<<(M + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const bf16*)dz, ld, M, C, db);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_l1(const float* base, const float* r, const float* target, int M, float* loss_sum, void* dr, float scale,
+               void* stream) {
+    k_l1<<<grid_of(M), 256, 0, (cudaStream_t)stream>>>(base, r, target, M, loss_sum, (bf16*)dr, scale);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_residual(const float* base, const float* r, int n, float* out, void* stream) {
+    k_residual<<<grid_of(n), 256, 0, (cudaStream_t)stream>>>(base, r, n, out);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_adam(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps, int t,
+                 void* wb, void* stream) {
+    const float c1 = 1.0f - powf(b1, (float)t), c2 = 1.0f - powf(b2, (float)t);
+    k_adam<<<grid_of(n), 256, 0, (cudaStream_t)stream>>>(w, g, m, v, n, lr, b1, b2, eps, c1, c2, (bf16*)wb);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_to_bf16(const float* src, int lds, int rows, int cols, void* dst, int ldd, void* stream) {
+    k_to_bf16<<<grid_of((long)rows * ldd), 256, 0, (cudaStream_t)stream>>>(src, lds, rows, cols, (bf16*)dst, ldd);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_pack(const void* accum, const float* feat, int P, void* x, float* base, void* stream) {
+    k_pack<<<grid_of(P), 256, 0, (cudaStream_t)stream>>>((const float4*)accum, feat, P, (bf16*)x, base);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_crop(const void* x, const float* base, const float* target, int H, int W, const int* crops, int B, int ch,
+                 int cw, void* xb, float* baseb, float* targetb, void* stream) {
+    k_crop<<<grid_of((long)B * ch * cw), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, base, target, H, W, crops, B, ch,
+                                                                          cw, (bf16*)xb, baseb, targetb);
     return (int)cudaGetLastError();
 }
 

@@ -85,6 +85,8 @@ void launch_particles(const FrameConst& fc, const float4* rec, const float* lut,
 void launch_primitive(const FrameConst& fc, const float4* rec, const uint2* cdesc, const float* lut,
                       uint32_t first_seed, uint32_t E, unsigned long long* sub, EnsTotal* etot,
                       unsigned long long* stats, cudaStream_t st);
+void launch_features(const FrameConst& fc, const unsigned long long* sub, const EnsTotal* etot, const float4* colour,
+                     uint32_t E, float* feat, cudaStream_t st);
 void launch_resolve(const FrameConst& fc, const unsigned long long* sub, const EnsTotal* etot, const float4* colour,
                     uint32_t E, float4* accum, unsigned long long* stats, cudaStream_t st);
 void launch_add_stat(unsigned long long* stats, int word, unsigned long long v, cudaStream_t st);

@@ -734,6 +734,55 @@ void launch_resolve(const FrameConst& fc, const unsigned long long* sub, const E
     k_resolve<<<(P + 255) / 256, 256, 0, st>>>(fc, sub, etot, colour, E, accum, stats);
 }
 
+// Denoiser features of the batch's ensembles (no counterpart in the reference, which has no
+// denoiser): per pixel and ensemble the resolved colour c (as k_resolve computes it), the covered
+// fraction alpha of its subpixels and the covered subpixels' depth sum / S; adds (c.r^2, c.g^2,
+// c.b^2, alpha, depth) to feat[pix * 8 + 0..4]. Skipped ensembles add nothing.
+__global__ void __launch_bounds__(256) k_features(FrameConst f, const ull* __restrict__ sub,
+                                                   const EnsTotal* __restrict__ etot, const float4* __restrict__ colour,
+                                                   uint32_t E, float* feat) {
+    uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t P = f.W * f.H;
+    if (pix >= P) return;
+    const uint32_t S = f.S;
+    const uint64_t PS = (uint64_t)P * S;
+    float q[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (uint32_t e = 0; e < E; ++e) {
+        if (__ldg(&etot[e].flags) != 0u) continue;
+        const ull* s = sub + (size_t)e * PS + (size_t)pix * S;
+        float sx = F_(0.0), sy = F_(0.0), sz = F_(0.0), cov = 0.0f, dep = 0.0f;
+        for (uint32_t k = 0; k < S; ++k) {
+            ull v = __ldcs(s + k);
+            uint32_t key = (uint32_t)(v >> 32), id = (uint32_t)v;
+            if (key == gxc::kEmpty || id == gxc::kEmpty) {
+                sx = sx + f.bg[0]; sy = sy + f.bg[1]; sz = sz + f.bg[2];
+            } else {
+                float4 c = __ldg(&colour[id]);
+                sx = sx + c.x; sy = sy + c.y; sz = sz + c.z;
+                cov += 1.0f;
+                dep += __uint_as_float(key & 0x7FFFFFFFu);
+            }
+        }
+        const float Sf = (float)S;
+        const float cr = div_(sx, Sf), cg = div_(sy, Sf), cb = div_(sz, Sf);
+        q[0] += cr * cr;
+        q[1] += cg * cg;
+        q[2] += cb * cb;
+        q[3] += cov / Sf;
+        q[4] += dep / Sf;
+    }
+    float* o = feat + (size_t)pix * 8;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) o[j] += q[j];
+}
+
+void launch_features(const FrameConst& fc, const unsigned long long* sub, const EnsTotal* etot, const float4* colour,
+                     uint32_t E, float* feat, cudaStream_t st) {
+    const uint32_t P = fc.W * fc.H;
+    if (P == 0 || E == 0) return;
+    k_features<<<(P + 255) / 256, 256, 0, st>>>(fc, sub, etot, colour, E, feat);
+}
+
 __global__ void k_add_stat(ull* stats, int word, ull v) { stats[word] += v; }
 void launch_add_stat(unsigned long long* stats, int word, unsigned long long v, cudaStream_t st) {
     k_add_stat<<<1, 1, 0, st>>>(stats, word, v);

@@ -56,6 +56,7 @@ struct DevBuf {
 
 struct gpsb_renderer {
     int device = 0;
+    float* feat = nullptr;  // caller-owned denoiser feature sums (W*H*8 floats), or null
     cudaStream_t own = nullptr, stream = nullptr;
     uint32_t W = 0, H = 0, side = 1;
     uint32_t n = 0, sh_max_degree = 0, sh_stride = 0;
@@ -297,6 +298,12 @@ static gpsb_status render_batch(gpsb_renderer* r, const FrameConst& f, bool part
         launch_resolve(f, r->sub.as<ull_t>(), r->etot.as<EnsTotal>(), r->colour.as<float4>(), E, accum, stats,
                        r->stream);
         CK(r, cudaGetLastError(), "resolve kernel");
+        if (r->feat) {
+            sc.kernels(1);
+            launch_features(f, r->sub.as<ull_t>(), r->etot.as<EnsTotal>(), r->colour.as<float4>(), E, r->feat,
+                            r->stream);
+            CK(r, cudaGetLastError(), "feature kernel");
+        }
     }
     r->last_batch = E;
     r->last_particle = particles;
@@ -460,6 +467,12 @@ void gpsb_destroy(gpsb_renderer* r) {
     delete r;
 }
 
+gpsb_status gpsb_set_feature_accum(gpsb_renderer* r, float* feat_dev) {
+    if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
+    r->feat = feat_dev;
+    return GPSB_OK;
+}
+
 gpsb_status gpsb_set_stream(gpsb_renderer* r, void* s) {
     if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
     cudaSetDevice(r->device);
@@ -561,6 +574,7 @@ gpsb_status gpsb_resize(gpsb_renderer* r, uint32_t w, uint32_t h, uint32_t spp_s
     r->W = w;
     r->H = h;
     r->side = spp_side;
+    r->feat = nullptr;  // sized for the old frame
     r->sub.release();
     r->accum.release();
     gpsb_status s = alloc_frame(r);

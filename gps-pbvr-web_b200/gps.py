@@ -406,6 +406,10 @@ class GpsRenderer:
         self._ck(self._L.gpsb_debug_read_subpixels(self._r, slot, out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def set_feature_accum(self, feat):
+        """Denoiser feature sums into `feat` (a zeroed CUDA tensor of W*H*8 float32), or None to stop."""
+        self._ck(self._L.gpsb_set_feature_accum(self._r, C.c_void_p(feat.data_ptr()) if feat is not None else None))
+
     def debug_error_word(self) -> int:
         return self._L.gpsb_debug_error_word(self._r)
 

@@ -169,6 +169,12 @@ gpsb_status gpsb_create(int device, uint32_t width, uint32_t height, uint32_t sp
 void gpsb_destroy(gpsb_renderer* r);
 /* Run the renderer's work on an external cudaStream_t (NULL restores its own stream). */
 gpsb_status gpsb_set_stream(gpsb_renderer* r, void* cuda_stream);
+/* Denoiser features (no counterpart in the reference, which has no denoiser): with feat_dev set
+ * (device memory of the caller, width*height*8 floats, zeroed by the caller), every rendered
+ * ensemble also adds, per pixel, (r^2, g^2, b^2, alpha, depth) of its resolved colour, covered
+ * subpixel fraction and covered depth sum / subpixels to feat_dev[pixel*8 + 0..4]. NULL turns it
+ * off; gpsb_resize turns it off. */
+gpsb_status gpsb_set_feature_accum(gpsb_renderer* r, float* feat_dev);
 
 /* ------------------------------------------------------------------- scene */
 /* GpsRenderer::set_gaussians (gps.rs:683). Host pointer. On error the old scene stays. */
@@ -307,6 +313,53 @@ gpsb_status gpsb_p0_sample(gpsb_renderer* r, uint32_t seed, uint32_t pixel_base,
 gpsb_status gpsb_sort_pairs_noalloc(uint32_t* keys_in, uint32_t* vals_in, uint32_t* keys_out,
                                     uint32_t* vals_out, uint32_t n, uint32_t key_bits,
                                     void* cuda_stream, uint32_t* err_dev);
+
+/* ------------------------------------------------------------------- denoiser kernels
+ * The learned denoiser of few-ensemble frames (BASELINE's "denoised batch vs plain"). The
+ * reference has no denoiser, so none of these has a counterpart in it. All pointers are device
+ * memory; activations are NHWC (pixel-major, channels innermost) bf16 with channel counts padded
+ * to multiples of 8; weights are (cout, kp) bf16 rows, k = (ky*3 + kx)*cin + ci, kp a multiple of
+ * 64 >= 9*cin. Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream); the
+ * return value is a cudaError_t code (0 = launched). `err` (a device word) receives a non-zero
+ * bit when a bounded device-side wait gives up. */
+/* y[p][ooff+n] = act(bias[n] + sum_k xcol[p][k] w[n][k]): 3x3 convolution, stride 1, zero padding
+ * 1, on the tcgen05 tensor cores; out is bf16, or fp32 when out_f32; relu != 0 applies ReLU. */
+int gpsb_dn_conv_fwd(const void* x, int ldx, int xoff, int cin, int B, int H, int W, const void* w, int cout,
+                     int kp, const float* bias, void* out, int ldo, int ooff, int out_f32, int relu,
+                     void* stream, uint32_t* err);
+/* dw[co][k] += sum_p dy[p][co] * xcol[p][k] (fp32, caller-zeroed): the weight gradient. */
+int gpsb_dn_conv_dw(const void* dy, int ldy, const void* x, int ldx, int xoff, int cin, int B, int H, int W,
+                    int cout, int kp, float* dw, void* stream, uint32_t* err);
+/* wf[ci][(8 - t)*coutp + co] = w[co][t*cin + ci]: weights of the data gradient (a forward conv). */
+int gpsb_dn_flip(const void* w, int cout, int cin, int kp, void* wf, int coutp, int kp2, void* stream);
+/* out[m][c] = g[m][goff+c] * (y[m][yoff+c] > 0) as bf16 (y NULL: no mask), zero for C <= c < ldo. */
+int gpsb_dn_relu_bwd(const float* g, int ldg, int goff, const void* y, int ldy, int yoff, int M, int C, void* out,
+                     int ldo, void* stream);
+/* nearest 2x upsampling into a channel slice, and its gradient (sum over 2x2 blocks). */
+int gpsb_dn_up2(const void* src, int lds, int B, int h, int w, int C, void* dst, int ldd, int doff, void* stream);
+int gpsb_dn_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int C, float* out, void* stream);
+/* 2x2 average pooling of a channel slice, and its gradient added into a channel slice. */
+int gpsb_dn_pool2(const void* src, int lds, int soff, int B, int h, int w, int C, void* dst, void* stream);
+int gpsb_dn_pool2_bwd_add(const float* g, int B, int h, int w, int C, float* acc, int lda, int aoff,
+                          void* stream);
+/* db[c] += sum over M pixels of dz[m][c] (bf16 dz, C <= 256). */
+int gpsb_dn_bias_grad(const void* dz, int ld, int M, int C, float* db, void* stream);
+/* L1 loss of base + r against target (M x 3 fp32): loss_sum += sum |d|; dr (M x 8 bf16) = scale*sign(d). */
+int gpsb_dn_l1(const float* base, const float* r, const float* target, int M, float* loss_sum, void* dr,
+               float scale, void* stream);
+/* out = base + r (n floats). */
+int gpsb_dn_residual(const float* base, const float* r, int n, float* out, void* stream);
+/* Adam step t (>= 1) on n fp32 weights w with gradient g and moments m, v; wb (optional) gets bf16 w. */
+int gpsb_dn_adam(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
+                 int t, void* wb, void* stream);
+/* dst[r][c] = bf16(c < cols ? src[r*lds + c] : 0) for c < ldd. */
+int gpsb_dn_to_bf16(const float* src, int lds, int rows, int cols, void* dst, int ldd, void* stream);
+/* Denoiser input of a frame: accum (P float4: rgb sum, count) and feature sums (P x 8 floats of
+ * gpsb_set_feature_accum, or NULL) -> x (P x 8 bf16) and base (P x 3 fp32 mean colour). */
+int gpsb_dn_pack(const void* accum, const float* feat, int P, void* x, float* base, void* stream);
+/* Training crops: crops[3b..3b+2] = (image, y0, x0) windows of ch x cw from N stacked H x W frames. */
+int gpsb_dn_crop(const void* x, const float* base, const float* target, int H, int W, const int* crops, int B,
+                 int ch, int cw, void* xb, float* baseb, float* targetb, void* stream);
 
 /* ------------------------------------------------------------------- PLY (gps-io) */
 /* load_ply (crates/gps-io/src/lib.rs:260-338) + activation (lib.rs:84-96) +
