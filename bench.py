@@ -15,6 +15,7 @@ gps-core's render_particles_3d, oracle/o1_core.cpp) on the host cores, on rank 0
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -272,6 +273,62 @@ def micro_scan_sort(pkg, r, stream, peak):
     return out
 
 
+def denoise_measure(pkg, r, stream, cams, p, per_view_ms, ref_ens=256):
+    """BASELINE's "ms to PSNR vs the 256-ensemble reference: denoised batch vs plain", per view:
+    the 4-ensemble frame through the trained denoiser (committed weights) against the plain
+    accumulation. PSNR (peak 1, linear RGB clamped to [0, 1]) against a 256-ensemble reference with
+    disjoint seeds; the plain path's PSNR is measured at 4..128 ensembles and the ensembles it
+    needs to match the denoised PSNR come from its fitted error model MSE(N) = s2 (1/N + 1/256);
+    times are ensembles x the view's ms per ensemble of this run, plus the denoiser's GPU time."""
+    import torch
+    from gps_pbvr_web_b200 import denoise as dn
+    from gps_pbvr_web_b200 import denoise_train as T
+    net = dn.Denoiser()
+    gate = dn.load_weights(net)
+    out = {"weights": "gps-pbvr-web_b200/weights/denoiser_pbvr_c3r.npz", "reference_ensembles": ref_ens,
+           "input_ensembles": 4, "views": {}}
+    P = W * H
+    with torch.cuda.stream(stream):
+        for name, cam in cams:
+            r.reset_accum()
+            r.render_ensembles(cam, p, 5_000_000, ref_ens)
+            ref = T.mean_rgb(torch.from_numpy(r.read_accum()).cuda())
+            feat = torch.zeros(P * 8, device="cuda")
+            r.reset_accum()
+            r.set_feature_accum(feat)
+            r.render_ensembles(cam, p, 6_000_000, 4)
+            r.set_feature_accum(None)
+            acc = torch.from_numpy(r.read_accum()).cuda()
+            x = torch.zeros(P, 8, dtype=torch.bfloat16, device="cuda")
+            base = torch.zeros(P, 3, device="cuda")
+            dn.pack(acc, feat, x, base)
+            ok, check = T.variance_gate(x, gate)
+            net.forward(x.view(1, H, W, 8), base.view(1, H, W, 3))  # warm-up
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(5):
+                pred = net.forward(x.view(1, H, W, 8), base.view(1, H, W, 3))
+            b.record(stream)
+            torch.cuda.synchronize()
+            dn_ms = a.elapsed_time(b) / 5
+            ps_dn, me_dn = T.psnr(pred.reshape(P, 3), ref)
+            prog = T.progressive(r, cam, p, 6_000_000, [4, 8, 16, 32, 64, 128])
+            curve = {n: T.psnr(T.mean_rgb(v), ref)[0] for n, v in prog.items()}
+            s2 = T.noise_model(curve, ref_ens)
+            n_same = T.n_model(s2, ref_ens, ps_dn)
+            ms_ens = per_view_ms[name]
+            frame_ms = 4 * ms_ens + dn_ms
+            out["views"][name] = {
+                "psnr_denoised": ps_dn, "maxerr_denoised": me_dn, "psnr_plain": curve,
+                "psnr_ceiling_vs_reference": 10.0 * math.log10(ref_ens / s2), "variance_check_passed": ok,
+                "denoiser_ms": dn_ms, "denoised_frame_ms": frame_ms,
+                "plain_ensembles_for_same_psnr": n_same,
+                "plain_ms_for_same_psnr": None if n_same is None else n_same * ms_ens,
+                "speedup_at_same_psnr": None if n_same is None else n_same * ms_ens / frame_ms,
+                "reaches_40db": {"denoised": ps_dn >= 40.0, "plain_max_measured": max(curve.values()) >= 40.0}}
+    return out
+
+
 def _time_events(fn, stream, warmup, reps):
     import torch
     for _ in range(warmup):
@@ -414,6 +471,10 @@ def run_b200(args, rank, world):
     if rank == 0 and not args.no_micro:
         prims = micro_scan_sort(pkg, r, stream, peak)
 
+    dnz = None
+    if rank == 0 and not args.no_denoise:
+        dnz = denoise_measure(pkg, r, stream, cams, p, per_view)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cams = cameras(pkg)
@@ -441,7 +502,7 @@ def run_b200(args, rank, world):
                                    "list_entries": st.list_entries / args.steps,
                                    "truncated_splats": st.truncated_splats / args.steps,
                                    "skipped_ensembles": st.skipped_ensembles},
-                "primitives": prims, "e2e": e2e, "cpu_baseline": cpu}
+                "primitives": prims, "denoise": dnz, "e2e": e2e, "cpu_baseline": cpu}
         print(json.dumps(line))
     r.close()
     if dist is not None:
@@ -459,6 +520,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-micro", action="store_true", help="skip the scan/sort HBM measurements")
+    ap.add_argument("--no-denoise", action="store_true", help="skip the denoised-vs-plain PSNR measurement")
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64)
     ap.add_argument("--views", default="near,mid,far", help="subset of the views (small profiling cases)")
     ap.add_argument("--ensembles", type=int, default=ENS, help="ensembles per view (small profiling cases)")

@@ -128,7 +128,7 @@ SIGNATURES = {
     "gpsb_dn_adam": (ST, [P, P, P, P, ST, C.c_float, C.c_float, C.c_float, C.c_float, ST, P, P]),
     "gpsb_dn_to_bf16": (ST, [P, ST, ST, ST, P, ST, P]),
     "gpsb_dn_pack": (ST, [P, P, ST, P, P, P]),
-    "gpsb_dn_crop": (ST, [P, P, P, ST, ST, P, ST, ST, ST, P, P, P, P]),
+    "gpsb_dn_crop": (ST, [P, P, P, ST, ST, ST, P, ST, ST, ST, P, P, P, P, P]),
 }
 
 _lib = None

@@ -336,13 +336,20 @@ __global__ void k_pack(const float4* accum, const float* feat, int P, bf16* x, f
 }
 
 // Training batch: crop b takes the ch x cw window at (y0, x0) of image img from the stacked frames
-// (x: N x H x W x 8 bf16, base and target: N x H x W x 3 fp32); crops[b] = (img, y0, x0).
-__global__ void k_crop(const bf16* x, const float* base, const float* target, int H, int W, const int* crops, int B,
-                       int ch, int cw, bf16* xb, float* baseb, float* targetb) {
+// (x: N x H x W x 8 bf16, base and target: N x H x W x 3 fp32); crops[b] = (img, y0, x0). A window
+// outside the frames gives zeros and sets bit 16 of *err.
+__global__ void k_crop(const bf16* x, const float* base, const float* target, int N, int H, int W, const int* crops,
+                       int B, int ch, int cw, bf16* xb, float* baseb, float* targetb, uint32_t* err) {
     const int i = gtid();
     if (i >= B * ch * cw) return;
     const int b = i / (ch * cw), yx = i - b * ch * cw, y = yx / cw, xq = yx - y * cw;
     const int img = crops[3 * b], y0 = crops[3 * b + 1], x0 = crops[3 * b + 2];
+    if (img < 0 || img >= N || y0 < 0 || y0 + ch > H || x0 < 0 || x0 + cw > W) {
+        *reinterpret_cast<uint4*>(xb + (size_t)i * 8) = make_uint4(0u, 0u, 0u, 0u);
+        for (int c = 0; c < 3; ++c) baseb[(size_t)i * 3 + c] = targetb[(size_t)i * 3 + c] = 0.0f;
+        if (yx == 0 && err) atomicOr(err, 1u << 16);
+        return;
+    }
     const size_t src = ((size_t)img * H + y0 + y) * W + x0 + xq;
     *reinterpret_cast<uint4*>(xb + (size_t)i * 8) = *reinterpret_cast<const uint4*>(x + src * 8);
 #pragma unroll
@@ -477,10 +484,10 @@ int gpsb_dn_pack(const void* accum, const float* feat, int P, void* x, float* ba
     k_pack<<<grid_of(P), 256, 0, (cudaStream_t)stream>>>((const float4*)accum, feat, P, (bf16*)x, base);
     return (int)cudaGetLastError();
 }
-int gpsb_dn_crop(const void* x, const float* base, const float* target, int H, int W, const int* crops, int B, int ch,
-                 int cw, void* xb, float* baseb, float* targetb, void* stream) {
-    k_crop<<<grid_of((long)B * ch * cw), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, base, target, H, W, crops, B, ch,
-                                                                          cw, (bf16*)xb, baseb, targetb);
+int gpsb_dn_crop(const void* x, const float* base, const float* target, int N, int H, int W, const int* crops, int B,
+                 int ch, int cw, void* xb, float* baseb, float* targetb, void* stream, uint32_t* err) {
+    k_crop<<<grid_of((long)B * ch * cw), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, base, target, N, H, W, crops, B,
+                                                                          ch, cw, (bf16*)xb, baseb, targetb, err);
     return (int)cudaGetLastError();
 }
 

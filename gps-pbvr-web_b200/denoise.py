@@ -3,6 +3,7 @@ forward and backward passes run on the library's tcgen05 kernels (csrc/denoise.c
 weights and activations and FP32 accumulation. PyTorch tensors only hold device memory here.
 """
 import ctypes as C
+import os
 
 from . import abi
 
@@ -275,8 +276,59 @@ def pack(accum, feat, x, base):
     _ck(_L().gpsb_dn_pack(_p(accum), _p(feat), P, _p(x), _p(base), _stream()), "pack")
 
 
-def crop(x, base, target, crops, ch, cw, xb, baseb, targetb):
-    """Training batch of crops[b] = (image, y0, x0) windows of ch x cw from stacked frames."""
+def crop(x, base, target, crops, ch, cw, xb, baseb, targetb, err=None):
+    """Training batch: crops (B, 3) int32 CUDA tensor of (image, y0, x0) windows of ch x cw taken
+    from the stacked frames x (N, H, W, 8), base and target (N, H, W, 3) into xb, baseb, targetb."""
     N, H, W, _ = x.shape
-    _ck(_L().gpsb_dn_crop(_p(x), _p(base), _p(target), H, W, _p(crops), crops.shape[0], ch, cw, _p(xb), _p(baseb),
-                          _p(targetb), _stream()), "crop")
+    if crops.dim() != 2 or crops.shape[1] != 3 or xb.shape[0] != crops.shape[0]:
+        raise ValueError("crops must be (B, 3) with B the batch of xb")
+    _ck(_L().gpsb_dn_crop(_p(x), _p(base), _p(target), N, H, W, _p(crops), crops.shape[0], ch, cw, _p(xb), _p(baseb),
+                          _p(targetb), _stream(), _p(err)), "crop")
+
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "denoiser_pbvr_c3r.npz")
+
+
+def load_weights(net, path=WEIGHTS):
+    """Loads weights saved by denoise_train.save_weights; returns the variance-gate limit."""
+    import numpy as np
+    import torch
+    z = np.load(path)
+    sd = {}
+    for n, q in net.p.items():
+        w = torch.zeros(q["cout"], q["kp"])
+        wr = torch.from_numpy(z[f"{n}.w"])
+        w[:, :wr.shape[1]] = wr
+        sd[n] = {"w": w, "b": torch.from_numpy(z[f"{n}.b"])}
+    net.load_state_dict(sd)
+    return float(z["gate_limit"])
+
+
+def render_denoised(renderer, net, cam, params, first_seed, *, ensembles=4, gate_limit, fallback_ensembles=64):
+    """A frame of `renderer` (a GpsRenderer) from few ensembles through the denoiser, or, when the
+    per-frame variance check fails (mean per-pixel ensemble standard deviation above gate_limit,
+    i.e. outside what the network was trained on), the plain accumulation of fallback_ensembles.
+    Returns (rgb (H*W, 3) CUDA tensor, used_denoiser, check value)."""
+    import torch
+    w, h = renderer.size()
+    P = w * h
+    if h % 4 or w % 4:
+        raise ValueError("the denoiser needs width and height divisible by 4")
+    feat = torch.zeros(P * 8, device="cuda")
+    renderer.reset_accum()
+    renderer.set_feature_accum(feat)
+    try:
+        renderer.render_ensembles(cam, params, first_seed, ensembles)
+        renderer.wait_idle()
+    finally:
+        renderer.set_feature_accum(None)
+    acc = torch.from_numpy(renderer.read_accum()).cuda()
+    x = torch.zeros(P, 8, dtype=torch.bfloat16, device="cuda")
+    base = torch.zeros(P, 3, device="cuda")
+    pack(acc, feat, x, base)
+    check = float(x[:, 5].float().mean())
+    if check <= gate_limit:
+        return net.forward(x.view(1, h, w, 8), base.view(1, h, w, 3)).reshape(P, 3).clone(), True, check
+    renderer.render_ensembles(cam, params, first_seed + ensembles, fallback_ensembles - ensembles)
+    acc = torch.from_numpy(renderer.read_accum()).cuda()
+    return acc[:, :3] / acc[:, 3:4].clamp(min=1.0), False, check

@@ -357,9 +357,10 @@ int gpsb_dn_to_bf16(const float* src, int lds, int rows, int cols, void* dst, in
 /* Denoiser input of a frame: accum (P float4: rgb sum, count) and feature sums (P x 8 floats of
  * gpsb_set_feature_accum, or NULL) -> x (P x 8 bf16) and base (P x 3 fp32 mean colour). */
 int gpsb_dn_pack(const void* accum, const float* feat, int P, void* x, float* base, void* stream);
-/* Training crops: crops[3b..3b+2] = (image, y0, x0) windows of ch x cw from N stacked H x W frames. */
-int gpsb_dn_crop(const void* x, const float* base, const float* target, int H, int W, const int* crops, int B,
-                 int ch, int cw, void* xb, float* baseb, float* targetb, void* stream);
+/* Training crops: crops[3b..3b+2] = (image, y0, x0) windows of ch x cw from N stacked H x W frames
+ * (B crops); a window outside the frames gives zeros and sets bit 16 of *err. */
+int gpsb_dn_crop(const void* x, const float* base, const float* target, int N, int H, int W, const int* crops,
+                 int B, int ch, int cw, void* xb, float* baseb, float* targetb, void* stream, uint32_t* err);
 
 /* ------------------------------------------------------------------- PLY (gps-io) */
 /* load_ply (crates/gps-io/src/lib.rs:260-338) + activation (lib.rs:84-96) +
