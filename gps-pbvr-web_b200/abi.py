@@ -53,6 +53,30 @@ class TuningC(C.Structure):
                 ("particle_items", C.c_uint32), ("particle_blocks_per_sm", C.c_uint32), ("ensemble_batch", C.c_uint32)]
 
 
+class SessionStateC(C.Structure):
+    _fields_ = [("sorted_active", C.c_uint32), ("sorted_ok", C.c_uint32), ("moving_prefers_gps", C.c_uint32),
+                ("lod_moving", C.c_uint32), ("effective_per_frame", C.c_uint32), ("lod_n", C.c_uint32),
+                ("auto_density", C.c_float), ("history_epoch", C.c_uint32), ("frames_since_reset", C.c_uint32),
+                ("next_seed", C.c_uint32), ("ensemble_counter", C.c_uint32), ("slow_frames", C.c_uint32),
+                ("last_demand", C.c_uint64), ("ema_ms", C.c_double)]
+
+
+# gpsb_session_backend: the renderer calls of a frame-loop session
+BE_RENDER = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32)
+BE_SORTED = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32)
+BE_PROBE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+BE_CALL = C.CFUNCTYPE(C.c_int, C.c_void_p)
+BE_STATS = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p)
+BE_U32 = C.CFUNCTYPE(C.c_uint32, C.c_void_p)
+
+
+class SessionBackendC(C.Structure):
+    _fields_ = [("render_ensembles", BE_RENDER), ("render_sorted", BE_SORTED), ("probe_demand", BE_PROBE),
+                ("request_stats", BE_CALL), ("latest_stats", BE_STATS), ("stats_issued", BE_U32),
+                ("accumulated", BE_U32), ("submitted", BE_U32), ("reset_accum", BE_CALL), ("reset_stats", BE_CALL),
+                ("gaussian_count", BE_U32)]
+
+
 STAGES = ["geometry", "count_scan", "particles", "resolve", "clear", "primitive", "sorted", "composite"]
 
 
@@ -113,6 +137,17 @@ SIGNATURES = {
     "gpsb_sort_pairs": (ST, [P, P, P, P, P, U32, U32]),
     "gpsb_p0_sample": (ST, [P, U32, U32, U32, U32, P]),
     "gpsb_get_tuning": (ST, [P, P]),
+    "gpsb_session_create": (ST, [P, P]),
+    "gpsb_session_create_with_backend": (ST, [P, P, P]),
+    "gpsb_session_destroy": (None, [P]),
+    "gpsb_session_configure": (ST, [P, P, U32, U32]),
+    "gpsb_session_set_lod": (ST, [P, C.c_int, C.c_double, U32]),
+    "gpsb_session_set_point_budget": (ST, [P, C.c_double]),
+    "gpsb_session_set_render_path": (ST, [P, U32, C.c_double]),
+    "gpsb_session_set_camera": (ST, [P, P, C.c_int]),
+    "gpsb_session_reset": (ST, [P]),
+    "gpsb_session_frame": (ST, [P, C.c_double, P]),
+    "gpsb_session_read_state": (ST, [P, P]),
     # denoiser kernels (return cudaError_t codes)
     "gpsb_dn_conv_fwd": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, ST, P, P, ST, ST, ST, ST, P, P]),
     "gpsb_dn_conv_dw": (ST, [P, ST, P, ST, ST, ST, ST, ST, ST, ST, ST, P, P, P]),

@@ -30,33 +30,6 @@ struct ConvFwd {
     int ldo, ooff, out_f32, relu;
     uint32_t* err;
 
-    __device__ __forceinline__ void load_a(uint8_t* tile, int m0, int k0) const {
-        const int M = B * H * W, K = 9 * cin;
-#pragma unroll 2
-        for (int c = threadIdx.x; c < umma::kBM * 8; c += umma::kThreads) {
-            const int r8 = c & 7, kc = (c >> 3) & 7, rg = c >> 6;
-            const int row = rg * 8 + r8, m = m0 + row, k = k0 + kc * 8;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (m < M && k < K) {
-                const int tap = k / cin, ci = k - tap * cin;
-                const int xq = m % W, yq = (m / W) % H, b = m / (W * H);
-                const int yy = yq + tap / 3 - 1, xx = xq + tap % 3 - 1;
-                if (yy >= 0 && yy < H && xx >= 0 && xx < W)
-                    v = __ldg(reinterpret_cast<const uint4*>(x + ((size_t)(b * H + yy) * W + xx) * ldx + xoff + ci));
-            }
-            *reinterpret_cast<uint4*>(tile + c * 16) = v;
-        }
-    }
-    template <int BN>
-    __device__ __forceinline__ void load_b_t(uint8_t* tile, int n0, int k0) const {
-        for (int c = threadIdx.x; c < BN * 8; c += umma::kThreads) {
-            const int r8 = c & 7, kc = (c >> 3) & 7, rg = c >> 6;
-            const int n = n0 + rg * 8 + r8, k = k0 + kc * 8;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (n < cout && k < kp) v = __ldg(reinterpret_cast<const uint4*>(w + (size_t)n * kp + k));
-            *reinterpret_cast<uint4*>(tile + c * 16) = v;
-        }
-    }
     __device__ __forceinline__ void epilogue(int m0, int n0, int row, int col0, const float* v) const {
         const int m = m0 + row;
         if (m >= B * H * W) return;
@@ -73,14 +46,58 @@ struct ConvFwd {
     }
 };
 
+// Asynchronous loader of the forward convolution: every thread owns 8 rows (pixels) of the A tile
+// and one 8-channel chunk column per K step; the pixels' coordinates are decoded once per tile and
+// each 16-byte chunk is a cp.async with zero fill (src-size 0) for padding taps and tails.
 template <int BN>
 struct ConvFwdN : ConvFwd {
-    __device__ __forceinline__ void load_b(uint8_t* tile, int n0, int k0) const { load_b_t<BN>(tile, n0, k0); }
+    int pix[8], py[8], px[8];
+
+    __device__ __forceinline__ void prepare(int m0, int) {
+        const int M = B * H * W, tid = threadIdx.x;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int row = 8 * ((tid >> 6) + 2 * i) + (tid & 7), m = m0 + row;
+            pix[i] = m;
+            if (m < M) {
+                px[i] = m % W;
+                py[i] = (m / W) % H;
+            } else {
+                px[i] = 0;
+                py[i] = -4;  // never inside the image
+            }
+        }
+    }
+    __device__ __forceinline__ void issue(uint8_t* a_tile, uint8_t* b_tile, int k0) const {
+        const int tid = threadIdx.x, K = 9 * cin;
+        const int k = k0 + ((tid >> 3) & 7) * 8;
+        const bool kok = k < K;
+        const int tap = kok ? k / cin : 0, ci = k - tap * cin;
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int yy = py[i] + dy, xx = px[i] + dx;
+            const bool ok = kok && yy >= 0 && yy < H && xx >= 0 && xx < W;
+            const bf16* src = ok ? x + (size_t)(pix[i] + dy * W + dx) * ldx + xoff + ci : x;
+            umma::cp_async16(a_tile + (tid + umma::kThreads * i) * 16, src, ok ? 16u : 0u);
+        }
+        for (int c = tid; c < BN * 8; c += umma::kThreads) {
+            const int n = n0_ + (c >> 6) * 8 + (c & 7), kk = k0 + ((c >> 3) & 7) * 8;
+            const bool ok = n < cout && kk < kp;
+            umma::cp_async16(b_tile + c * 16, ok ? w + (size_t)n * kp + kk : w, ok ? 16u : 0u);
+        }
+    }
+    int n0_ = 0;
 };
 
 template <int BN>
+__host__ __device__ constexpr int fwd_stages() { return BN >= 128 ? 3 : 4; }
+
+template <int BN>
 __global__ void __launch_bounds__(umma::kThreads) k_conv_fwd(ConvFwdN<BN> pb) {
-    umma::gemm_tile<BN>(pb, blockIdx.x * umma::kBM, blockIdx.y * BN, 0, pb.kp);
+    ConvFwdN<BN> q = pb;
+    q.n0_ = blockIdx.y * BN;
+    umma::gemm_tile_async<BN, fwd_stages<BN>()>(q, blockIdx.x * umma::kBM, blockIdx.y * BN, 0, pb.kp);
 }
 
 // ---------------------------------------------------------------------------- weight gradient
@@ -368,7 +385,7 @@ template <int BN>
 static cudaError_t launch_fwd(const ConvFwd& p, cudaStream_t st) {
     ConvFwdN<BN> q;
     static_cast<ConvFwd&>(q) = p;
-    const size_t smem = umma::smem_bytes<BN>();
+    const size_t smem = umma::smem_bytes_async<BN, fwd_stages<BN>()>();
     cudaFuncSetAttribute(k_conv_fwd<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int M = p.B * p.H * p.W;
     dim3 grid((M + umma::kBM - 1) / umma::kBM, (p.cout + BN - 1) / BN);

@@ -186,5 +186,109 @@ __device__ __forceinline__ void gemm_tile(const P& pb, int m0, int n0, int k_beg
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
 }
 
+// Issue one asynchronous 16-byte global -> shared copy; bytes < 16 zero-fills the rest (0: all zero).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr(dst)), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <int BN, int S>
+__host__ __device__ constexpr size_t smem_bytes_async() {
+    return (size_t)S * ((size_t)kBM * kBK * 2 + (size_t)BN * kBK * 2) + 128;
+}
+
+// The mainloop with S stages filled by asynchronous copies: P provides
+//   __device__ void prepare(int m0, int n0)                   // per-tile loader state (registers)
+//   __device__ void issue(uint8_t* a_tile, uint8_t* b_tile, int k0)   // cp.async of one K step
+//   __device__ void epilogue(...), err    (as gemm_tile)
+// Stage s is copied S-1 steps ahead; a stage is refilled only after the MMAs that read it have
+// completed (their mbarrier), and the tensor core reads a stage only after every thread's copies
+// into it have landed (cp.async.wait_group + proxy fence + barrier).
+template <int BN, int S, class P>
+__device__ __forceinline__ void gemm_tile_async(P& pb, int m0, int n0, int k_begin, int k_end) {
+    static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256 && S >= 2 && S <= 6, "shape");
+    extern __shared__ __align__(128) uint8_t s_raw[];
+    __shared__ __align__(8) uint64_t s_bar[S];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_raw) + 127) & ~(uintptr_t)127);
+    constexpr uint32_t kABytes = kBM * kBK * 2, kBBytes = BN * kBK * 2;
+    auto sa = [&](int b) { return base + b * kABytes; };
+    auto sb = [&](int b) { return base + S * kABytes + b * kBBytes; };
+    const int tid = threadIdx.x, warp = tid >> 5;
+    constexpr uint32_t kCols = tmem_cols<BN>();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&s_tmem)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < S; ++i) mbar_init(&s_bar[i]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    pb.prepare(m0, n0);
+    const int steps = (k_end - k_begin) / kBK;
+#pragma unroll
+    for (int i = 0; i < S - 1; ++i) {
+        if (i < steps) pb.issue(sa(i), sb(i), k_begin + i * kBK);
+        cp_async_commit();
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = s_tmem;
+    constexpr uint32_t idesc = idesc_bf16(BN);
+    for (int s = 0; s < steps; ++s) {
+        const int buf = s % S;
+        cp_async_wait<S - 2>();  // this thread's copies of stage s have landed
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        if (s_fail) break;
+        if (tid == 0) {
+            const uint32_t a0 = saddr(sa(buf)), b0 = saddr(sb(buf));
+#pragma unroll
+            for (int j = 0; j < kBK / 16; ++j)
+                mma_bf16(tmem, smem_desc(a0 + j * 256), smem_desc(b0 + j * 256), idesc, s > 0 || j > 0);
+            mma_commit(&s_bar[buf]);
+        }
+        // refill the stage read by step s-1 with step s+S-1, once those MMAs are done
+        const int nxt = s + S - 1;
+        if (nxt < steps) {
+            const int nb = nxt % S;
+            if (s >= 1 && !mbar_wait(&s_bar[nb], ((s - 1) / S) & 1)) s_fail = 1;
+            pb.issue(sa(nb), sb(nb), k_begin + nxt * kBK);
+        }
+        cp_async_commit();
+    }
+    cp_async_wait<0>();
+    bool ok = !s_fail;
+    const int last = steps - 1;
+    if (steps > 0 && ok) ok = mbar_wait(&s_bar[last % S], (last / S) & 1);
+    if (!ok) {
+        if (tid == 0) atomicOr(pb.err, GEMM_ERR_TIMEOUT);
+        if (steps > 0) mbar_wait(&s_bar[last % S], (last / S) & 1);
+    }
+    fence_after();
+    if (ok && steps > 0) {
+        const int row = warp * 32 + (tid & 31);
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+            pb.epilogue(m0, n0, row, c, v);
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+}
+
 }  // namespace umma
 }  // namespace gpsb

@@ -314,6 +314,55 @@ gpsb_status gpsb_sort_pairs_noalloc(uint32_t* keys_in, uint32_t* vals_in, uint32
                                     uint32_t* vals_out, uint32_t n, uint32_t key_bits,
                                     void* cuda_stream, uint32_t* err_dev);
 
+/* ------------------------------------------------------------------- frame-loop session
+ * The reference viewer's frame policy (crates/gps-web/src/lib.rs:437-697: Viewer::frame, set_lod,
+ * set_point_budget, set_render_path), headless: per tick it restarts the history when the
+ * camera, parameters or LOD state change, keeps the non-blocking statistics readback going,
+ * adapts the point-budget density factor, picks GPS particles or the depth-sorted path (Auto:
+ * demand probe of the still view, switch above the threshold with 0.5 hysteresis, hand motion
+ * to particles when sorting is slow), and renders the manual or adaptive number of ensembles
+ * (one while the camera moves, with the moving-camera particle cap). Half-resolution rendering
+ * (lib.rs:333-353) is gpsb_resize to ceil(w/2) x ceil(h/2) plus gpsb_composite_rgba8 at w x h. */
+typedef struct gpsb_session gpsb_session;
+/* The renderer calls a session makes (gpsb_session_create binds them to a gpsb_renderer). */
+typedef struct gpsb_session_backend {
+    gpsb_status (*render_ensembles)(void* ctx, const gpsb_camera* cam, const gpsb_params* p, uint32_t first_seed,
+                                    uint32_t count);
+    gpsb_status (*render_sorted)(void* ctx, const gpsb_camera* cam, const gpsb_params* p, uint32_t as_ensembles);
+    gpsb_status (*probe_demand)(void* ctx, const gpsb_camera* cam, const gpsb_params* p);
+    gpsb_status (*request_stats)(void* ctx);
+    gpsb_status (*latest_stats)(void* ctx, gpsb_stats* out);
+    uint32_t (*stats_issued)(void* ctx);
+    uint32_t (*accumulated)(void* ctx);
+    uint32_t (*submitted)(void* ctx);
+    gpsb_status (*reset_accum)(void* ctx);
+    gpsb_status (*reset_stats)(void* ctx);
+    uint32_t (*gaussian_count)(void* ctx);
+} gpsb_session_backend;
+typedef struct gpsb_session_state {
+    uint32_t sorted_active, sorted_ok, moving_prefers_gps, lod_moving;
+    uint32_t effective_per_frame, lod_n;
+    float auto_density;
+    uint32_t history_epoch, frames_since_reset, next_seed, ensemble_counter, slow_frames;
+    uint64_t last_demand;
+    double ema_ms;
+} gpsb_session_state;
+gpsb_status gpsb_session_create(gpsb_renderer* r, gpsb_session** out);
+gpsb_status gpsb_session_create_with_backend(const gpsb_session_backend* backend, void* ctx, gpsb_session** out);
+void gpsb_session_destroy(gpsb_session* s);
+/* parameters (density clamped to 0.01..100, cap >= 1), ensembles per tick (1..4) and target */
+gpsb_status gpsb_session_configure(gpsb_session* s, const gpsb_params* p, uint32_t per_frame, uint32_t target);
+gpsb_status gpsb_session_set_lod(gpsb_session* s, int adaptive, double target_ms, uint32_t moving_cap);
+gpsb_status gpsb_session_set_point_budget(gpsb_session* s, double millions);
+/* mode 0 GPS particles, 1 depth-sorted, 2 Auto (GPS method only; PBVR always uses particles) */
+gpsb_status gpsb_session_set_render_path(gpsb_session* s, uint32_t mode, double demand_threshold_millions);
+/* camera of the next ticks (a different camera restarts the history); user_input marks motion */
+gpsb_status gpsb_session_set_camera(gpsb_session* s, const gpsb_camera* cam, int user_input);
+gpsb_status gpsb_session_reset(gpsb_session* s);
+/* one tick at monotonic time now_ms; *presented = 1 when the accumulation changed */
+gpsb_status gpsb_session_frame(gpsb_session* s, double now_ms, int* presented);
+gpsb_status gpsb_session_read_state(const gpsb_session* s, gpsb_session_state* out);
+
 /* ------------------------------------------------------------------- denoiser kernels
  * The learned denoiser of few-ensemble frames (BASELINE's "denoised batch vs plain"). The
  * reference has no denoiser, so none of these has a counterpart in it. All pointers are device

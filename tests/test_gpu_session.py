@@ -1,0 +1,82 @@
+"""The frame-loop session on the real renderer: Auto path on a GPS scene converges to the target
+through the probe and the chosen path; PBVR through particles with adaptive LOD; and the
+half-resolution mode (render at ceil(w/2) x ceil(h/2), composite at w x h, lib.rs:333-353)."""
+import importlib
+
+import numpy as np
+import pytest
+
+from conftest import load_package
+
+pytestmark = pytest.mark.gpu
+PKG = load_package()
+S = importlib.import_module(PKG.__name__ + ".session")
+
+
+def _scene(r):
+    from gps_pbvr_web_b200 import scenes
+    splats, sh, deg = PKG.load_ply(scenes.cluster_scene(30_000, seed=2, degree=1))
+    r.set_gaussians_sh(splats, sh, deg)
+
+
+def test_session_auto_path_reaches_target():
+    W, H = 128, 96
+    r = PKG.GpsRenderer(W, H, 1)
+    _scene(r)
+    cam = PKG.OrbitCamera(target=(0.0, 0.0, 0.0), distance=4.0, yaw=0.4, pitch=0.2, up=(0.0, -1.0, 0.0),
+                          fov_y=0.9).to_camera(W, H)
+    s = S.FrameSession(renderer=r)
+    s.configure(PKG.RenderParams(spp_side=1, max_points_per_splat=4096), per_frame=4, target=16)
+    s.set_render_path(2, 0.1)  # a tiny threshold: the probe picks the sorted path
+    s.set_camera(cam)
+    t = 0.0
+    for _ in range(40):
+        t += 16.7
+        s.frame(t)
+        if r.accumulated() >= 16:
+            break
+    r.wait_idle()
+    assert r.accumulated() >= 16
+    assert s.state()["sorted_active"] == 1 and s.state()["last_demand"] > 0
+    s.close()
+    r.close()
+
+
+def test_session_pbvr_adaptive_lod():
+    W, H = 128, 96
+    r = PKG.GpsRenderer(W, H, 1)
+    _scene(r)
+    cam = PKG.OrbitCamera(target=(0.0, 0.0, 0.0), distance=6.0, yaw=0.4, pitch=0.2, up=(0.0, -1.0, 0.0),
+                          fov_y=0.9).to_camera(W, H)
+    p = PKG.RenderParams(spp_side=1, max_points_per_splat=4096, method=PKG.Method.Extinction)
+    s = S.FrameSession(renderer=r)
+    s.configure(p, per_frame=1, target=12)
+    s.set_lod(True, 33.3, 256)
+    s.set_camera(cam)
+    t = 0.0
+    for _ in range(60):
+        t += 5.0
+        s.frame(t)
+    r.wait_idle()
+    assert r.accumulated() == 12 and s.state()["sorted_active"] == 0
+    s.close()
+    r.close()
+
+
+def test_half_resolution_mode():
+    W, H = 161, 97
+    r = PKG.GpsRenderer(W, H, 1)
+    _scene(r)
+    w2, h2 = (W + 1) // 2, (H + 1) // 2
+    r.resize(w2, h2, 1)
+    cam = PKG.OrbitCamera(target=(0.0, 0.0, 0.0), distance=6.0, yaw=0.4, pitch=0.2, up=(0.0, -1.0, 0.0),
+                          fov_y=0.9).to_camera(w2, h2)
+    p = PKG.RenderParams(spp_side=1, max_points_per_splat=4096)
+    r.render_ensembles(cam, p, 1, 4)
+    img = np.asarray(r.composite(p, W, H))
+    assert img.size == W * H * 4
+    small = np.asarray(r.composite(p, w2, h2))
+    assert small.size == w2 * h2 * 4
+    # the upsampled frame is the bilinear magnification of the half-size one: same mean brightness
+    assert abs(img.reshape(-1, 4)[:, :3].astype(np.float64).mean() - small.reshape(-1, 4)[:, :3].astype(np.float64).mean()) < 4.0
+    r.close()
