@@ -191,4 +191,5 @@ def header_functions(header_path=None):
     path = header_path or os.path.join(os.path.dirname(HERE), "include", "gpsb200.h")
     text = open(path).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(gpsb_[a-z0-9_]+)\s*\(", text)))
+    # function names are followed by "(", function-pointer members of a struct by "(*"
+    return sorted(set(re.findall(r"\b(gpsb_[a-z0-9_]+)\s*\((?!\s*\*)", text)))
