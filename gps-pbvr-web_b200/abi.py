@@ -107,6 +107,7 @@ SIGNATURES = {
     "gpsb_reset_stats": (ST, [P]),
     "gpsb_render_ensembles": (ST, [P, P, P, U32, U32]),
     "gpsb_render_trajectory": (ST, [P, P, U32, P, U32, U32, P]),
+    "gpsb_render_trajectory_graph": (ST, [P, P, U32, P, U32, U32, P]),
     "gpsb_render_sorted": (ST, [P, P, P, U32]),
     "gpsb_probe_demand": (ST, [P, P, P]),
     "gpsb_read_accum": (ST, [P, P]),

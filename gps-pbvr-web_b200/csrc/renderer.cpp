@@ -99,6 +99,11 @@ struct gpsb_renderer {
     RadixScratch prim_sort;
     // launch-shape tuning
     uint32_t particle_items = 16, particle_blocks_per_sm = 5, ensemble_batch = 64;
+    // captured trajectory pipeline (gpsb_render_trajectory_graph) and the key of its work
+    cudaGraphExec_t traj_exec = nullptr;
+    std::vector<uint8_t> traj_key;
+    uint64_t traj_launches = 0;
+    uint64_t scene_gen = 0;
 };
 
 // Brackets the kernels of one stage with CUDA events on the renderer's stream (when profiling)
@@ -461,6 +466,7 @@ void gpsb_destroy(gpsb_renderer* r) {
         cudaEventDestroy(pe.b);
     }
     for (cudaEvent_t e : r->pool) cudaEventDestroy(e);
+    if (r->traj_exec) cudaGraphExecDestroy(r->traj_exec);
     if (r->stats_pinned) cudaFreeHost(r->stats_pinned);
     if (r->stats_event) cudaEventDestroy(r->stats_event);
     if (r->own) cudaStreamDestroy(r->own);
@@ -549,6 +555,7 @@ static gpsb_status set_scene(gpsb_renderer* r, const void* g, size_t n, const fl
     r->batch_cap = 0;
     r->sub.release(); r->clist.release(); r->lookback.release(); r->etot.release();
     r->have_sorted = false;
+    r->scene_gen += 1;
     return gpsb_reset_accum(r);
 }
 
@@ -631,6 +638,83 @@ gpsb_status gpsb_render_trajectory(gpsb_renderer* r, const gpsb_camera* cams, ui
         s = render_camera(r, &cams[c], p, first_seed, E, out);
         if (s != GPSB_OK) return s;
     }
+    return GPSB_OK;
+}
+
+// The trajectory's whole pipeline (per camera: clear, geometry, and per ensemble batch the count
+// + scan, the persistent particle kernel and the resolve) captured once into a CUDA graph and
+// replayed: a repeat with the same cameras, parameters, seeds, output, scene, resolution and
+// tuning launches the graph again without re-encoding; anything else re-captures.
+gpsb_status gpsb_render_trajectory_graph(gpsb_renderer* r, const gpsb_camera* cams, uint32_t n_cams,
+                                         const gpsb_params* p, uint32_t first_seed, uint32_t E, void* accum_out_dev) {
+    if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
+    if (n_cams == 0 || E == 0) return GPSB_OK;
+    if (!cams || !accum_out_dev || !p) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null cameras, parameters or output");
+    if (r->stream == nullptr) return fail(r, GPSB_ERR_STATE, "graph capture needs a non-default stream");
+    if (r->prof_on) return fail(r, GPSB_ERR_STATE, "stage profiling is on; use gpsb_render_trajectory");
+    if (r->feat) return fail(r, GPSB_ERR_STATE, "feature sums are on; use gpsb_render_trajectory");
+    cudaSetDevice(r->device);
+    for (uint32_t c = 0; c < n_cams; ++c) {
+        gpsb_status s = check_params(r, &cams[c], p);
+        if (s != GPSB_OK) return s;
+    }
+    // key of the captured work
+    std::vector<uint8_t> key;
+    auto put = [&](const void* d, size_t n) { key.insert(key.end(), (const uint8_t*)d, (const uint8_t*)d + n); };
+    put(cams, sizeof(gpsb_camera) * n_cams);
+    put(p, sizeof *p);
+    uint64_t misc[] = {first_seed, E, (uint64_t)(uintptr_t)accum_out_dev, r->scene_gen, r->W, r->H, r->side,
+                       r->particle_items, r->particle_blocks_per_sm, r->ensemble_batch, (uint64_t)r->sorted.digit_bits,
+                       (uint64_t)(uintptr_t)r->stream};
+    put(misc, sizeof misc);
+    // the device buffers baked into the graph: a reallocation (bigger batch, new scene or frame
+    // size) must re-capture, never replay stale pointers
+    const void* bufs[] = {r->splats.p, r->sh.p, r->lut.p, r->rec.p, r->cdesc.p, r->colour.p, r->stats.p, r->err.p,
+                          r->sub.p, r->clist.p, r->lookback.p, r->etot.p, r->counters.p};
+    put(bufs, sizeof bufs);
+    if (!r->traj_exec || key != r->traj_key) {
+        if (r->traj_exec) {
+            cudaGraphExecDestroy(r->traj_exec);
+            r->traj_exec = nullptr;
+        }
+        // every buffer the pipeline uses exists before the capture (no allocation inside it)
+        uint32_t B = pick_batch(r, E);
+        gpsb_status s = ensure_batch(r, B);
+        if (s != GPSB_OK) return s;
+        CK(r, r->counters.ensure(64), "counters");
+        // the buffers may have just been (re)allocated: key them as they are now
+        const void* now[] = {r->splats.p, r->sh.p, r->lut.p, r->rec.p, r->cdesc.p, r->colour.p, r->stats.p, r->err.p,
+                             r->sub.p, r->clist.p, r->lookback.p, r->etot.p, r->counters.p};
+        key.resize(key.size() - sizeof now);
+        put(now, sizeof now);
+        cudaGraph_t g = nullptr;
+        const uint64_t launches0 = r->total_launches;
+        CK(r, cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        const size_t P = (size_t)r->W * r->H;
+        gpsb_status st = GPSB_OK;
+        for (uint32_t c = 0; c < n_cams && st == GPSB_OK; ++c) {
+            float4* out = (float4*)accum_out_dev + (size_t)c * P;
+            if (cudaMemsetAsync(out, 0, P * 16, r->stream) != cudaSuccess) st = GPSB_ERR_CUDA;
+            if (st == GPSB_OK) st = render_camera(r, &cams[c], p, first_seed, E, out);
+        }
+        cudaError_t e = cudaStreamEndCapture(r->stream, &g);
+        if (st != GPSB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) return cuda_fail(r, e, "capture of the trajectory");
+        e = cudaGraphInstantiate(&r->traj_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            r->traj_exec = nullptr;
+            return cuda_fail(r, e, "graph instantiation");
+        }
+        r->traj_key = key;
+        r->traj_launches = r->total_launches - launches0;
+        r->total_launches = launches0;
+    }
+    CK(r, cudaGraphLaunch(r->traj_exec, r->stream), "graph launch");
+    r->total_launches += r->traj_launches;
     return GPSB_OK;
 }
 

@@ -333,6 +333,15 @@ class GpsRenderer:
         self._ck(self._L.gpsb_render_trajectory(self._r, arr, len(cams), C.byref(p), first_seed & 0xFFFFFFFF,
                                                 ensembles_per_camera, C.c_void_p(accum_out_ptr)))
 
+    def render_trajectory_graph(self, cams: Sequence[OracleCamera], params: RenderParams, first_seed: int,
+                                ensembles_per_camera: int, accum_out_ptr: int):
+        """render_trajectory through one captured CUDA graph (captured on the first call, relaunched
+        by identical repeats)."""
+        arr = (abi.Camera * len(cams))(*[c.to_c() for c in cams])
+        p = params.to_c()
+        self._ck(self._L.gpsb_render_trajectory_graph(self._r, arr, len(cams), C.byref(p), first_seed & 0xFFFFFFFF,
+                                                      ensembles_per_camera, C.c_void_p(accum_out_ptr)))
+
     def render_sorted(self, cam: OracleCamera, params: RenderParams, as_ensembles: int):
         c, p = cam.to_c(), params.to_c()
         self._ck(self._L.gpsb_render_sorted(self._r, C.byref(c), C.byref(p), as_ensembles))

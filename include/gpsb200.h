@@ -207,6 +207,15 @@ gpsb_status gpsb_render_ensembles(gpsb_renderer* r, const gpsb_camera* cam, cons
 gpsb_status gpsb_render_trajectory(gpsb_renderer* r, const gpsb_camera* cams, uint32_t n_cams,
                                    const gpsb_params* p, uint32_t first_seed,
                                    uint32_t ensembles_per_camera, void* accum_out_dev);
+/* The same trajectory through one captured CUDA graph (no counterpart in the reference, which
+ * encodes every pass per submit): the first call captures the whole pipeline of all cameras and
+ * ensemble batches on the renderer's stream and launches it; a repeat with identical cameras,
+ * parameters, seeds, output buffer, scene, frame size and tuning only relaunches the graph, any
+ * change re-captures. Needs a non-default stream (the renderer's own, or gpsb_set_stream with a
+ * created stream); refused while stage profiling or feature sums are on. */
+gpsb_status gpsb_render_trajectory_graph(gpsb_renderer* r, const gpsb_camera* cams, uint32_t n_cams,
+                                         const gpsb_params* p, uint32_t first_seed, uint32_t ensembles_per_camera,
+                                         void* accum_out_dev);
 /* render_sorted (gps.rs:930-944): depth-sorted alpha image written into the history with
  * count 1 and reported as `as_ensembles` accumulated ensembles. */
 gpsb_status gpsb_render_sorted(gpsb_renderer* r, const gpsb_camera* cam, const gpsb_params* p,

@@ -80,3 +80,58 @@ def test_half_resolution_mode():
     # the upsampled frame is the bilinear magnification of the half-size one: same mean brightness
     assert abs(img.reshape(-1, 4)[:, :3].astype(np.float64).mean() - small.reshape(-1, 4)[:, :3].astype(np.float64).mean()) < 4.0
     r.close()
+
+
+def test_trajectory_graph_matches_the_direct_path():
+    """The captured trajectory (16 orbit cameras x 3 ensembles) equals the directly encoded one
+    bit for bit, on the capture and on a replay; new seeds re-capture and still match."""
+    import torch
+    W, H = 96, 64
+    r = PKG.GpsRenderer(W, H, 1)
+    _scene(r)
+    st = torch.cuda.Stream()
+    r.set_stream(st.cuda_stream)
+    cams = [PKG.OrbitCamera(target=(0.0, 0.0, 0.0), distance=5.0, yaw=0.4 * k, pitch=0.2, up=(0.0, -1.0, 0.0),
+                            fov_y=0.9).to_camera(W, H) for k in range(16)]
+    p = PKG.RenderParams(spp_side=1, max_points_per_splat=4096, method=PKG.Method.Extinction)
+    a = torch.zeros(16 * W * H * 4, device="cuda")
+    b = torch.zeros_like(a)
+    r.render_trajectory(cams, p, 11, 3, a.data_ptr())
+    r.wait_idle()
+    for _ in range(2):
+        b.fill_(-1.0)
+        r.render_trajectory_graph(cams, p, 11, 3, b.data_ptr())
+        r.wait_idle()
+        assert torch.equal(a, b)
+    r.render_trajectory(cams, p, 40, 3, a.data_ptr())
+    r.render_trajectory_graph(cams, p, 40, 3, b.data_ptr())
+    r.wait_idle()
+    assert torch.equal(a, b) and r.debug_error_word() == 0
+    r.close()
+
+
+def test_autotuner_sweeps_and_shapes_do_not_change_results():
+    """The autotuner times every particle launch shape through the captured graph and returns the
+    fastest; every shape renders the same accumulation bit for bit."""
+    import torch
+    from gps_pbvr_web_b200 import autotune
+    W, H = 96, 64
+    r = PKG.GpsRenderer(W, H, 1)
+    _scene(r)
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        cams = [PKG.OrbitCamera(target=(0.0, 0.0, 0.0), distance=5.0, yaw=0.5 * k, pitch=0.2, up=(0.0, -1.0, 0.0),
+                                fov_y=0.9).to_camera(W, H) for k in range(2)]
+        p = PKG.RenderParams(spp_side=1, max_points_per_splat=4096, method=PKG.Method.Extinction)
+        best, results = autotune.tune(r, cams, p, ensembles=2, reps=2)
+        assert len(results) == len(autotune.PARTICLE_SPACE) and best in autotune.PARTICLE_SPACE
+        assert all(ms > 0 for _, ms in results)
+        outs = []
+        for shape in (autotune.PARTICLE_SPACE[0], autotune.PARTICLE_SPACE[-1], best):
+            r.set_tuning(**shape)
+            o = torch.zeros(2 * W * H * 4, device="cuda")
+            r.render_trajectory(cams, p, 3, 2, o.data_ptr())
+            r.wait_idle()
+            outs.append(o)
+        assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+    r.close()

@@ -206,3 +206,11 @@ def test_pbvr_never_uses_the_sorted_path():
         s.frame(16.7 * (k + 1))
     assert not any(c[0] in ("probe", "sorted") for c in f.calls)
     assert f.acc == 4
+
+
+def test_autotune_key_buckets():
+    at = importlib.import_module(PKG.__name__ + ".autotune")
+    assert at.key(560_000, 1280, 720, 2, False) == "m2-particle-1280x720-n524288"
+    assert at.key(2_000_000, 1920, 1080, 4, False) == "m4-particle-1920x1080-n2097152"
+    assert at.key(10_000, 256, 256, 0, True) == "m0-sorted-256x256-n8192"
+    assert len(at.PARTICLE_SPACE) == 9 and len(at.SORTED_SPACE) == 9
