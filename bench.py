@@ -343,6 +343,58 @@ def _time_events(fn, stream, warmup, reps):
     return a.elapsed_time(b) / reps
 
 
+def run_trajectory(args, rank, world):
+    """Configuration 3 (one line, not the default): the cluster generator scaled to 2,000,000
+    Gaussians (SH3) at 1920x1080, a 360-degree orbit of 16 cameras x E ensembles (distance 7)
+    rendered through one captured CUDA graph, for PBVR Extinction C3+R and ScreenOccupancy, with
+    the launch shape chosen by the autotuner (sweep on 2 cameras x 2 ensembles)."""
+    import torch
+    pkg = load_package()
+    from gps_pbvr_web_b200 import autotune, scenes
+    n, Wt, Ht, ncam = args.traj_gaussians, 1920, 1080, 16
+    splats, sh, deg = pkg.load_ply(scenes.cluster_scene(n, seed=0, degree=3))
+    stream = torch.cuda.Stream()
+    r = pkg.GpsRenderer(Wt, Ht, 1)
+    r.set_stream(stream.cuda_stream)
+    r.set_gaussians_sh(splats, sh, deg)
+    cams = [pkg.OrbitCamera(target=(0.0, 0.0, 0.0), distance=7.0, yaw=2 * math.pi * k / ncam, pitch=0.25,
+                            up=(0.0, -1.0, 0.0), fov_y=0.9).to_camera(Wt, Ht) for k in range(ncam)]
+    out = torch.zeros(ncam * Wt * Ht * 4, device="cuda")
+    E = args.ensembles
+    rows = {}
+    with torch.cuda.stream(stream):
+        for name, method in (("PBVR Extinction C3+R", pkg.Method.Extinction), ("ScreenOccupancy", pkg.Method.ScreenOccupancy)):
+            p = pkg.RenderParams(spp_side=1, max_points_per_splat=CAP, method=method)
+            if method == pkg.Method.Extinction:
+                p.pbvr.calibration = pkg.Calibration.PerSplatFootprint
+                p.pbvr.radial_correction = True
+            best, sweep = autotune.tune(r, cams[:2], p, ensembles=2, reps=2)
+            r.set_tuning(**best)
+            r.render_trajectory_graph(cams, p, 1, E, out.data_ptr())  # capture + warm-up
+            torch.cuda.synchronize()
+            l0 = r.profile()["total_launches"]
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                r.render_trajectory_graph(cams, p, 1, E, out.data_ptr())
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / args.steps
+            rows[name] = {"ms_per_trajectory": ms, "gpu_launches_per_trajectory": (r.profile()["total_launches"] - l0) / args.steps, "ensembles_per_s": ncam * E / (ms / 1e3),
+                          "ms_per_ensemble": ms / (ncam * E), "autotuned": best,
+                          "sweep_ms": [[sh_, round(t, 3)] for sh_, t in sweep]}
+    line = {"metric": "ensembles/s (trajectory, captured CUDA graph)", "value": rows["PBVR Extinction C3+R"]["ensembles_per_s"],
+            "unit": "ensembles/s", "n_gpus": 1, "steps": args.steps, "warmup": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": f"{n} synthetic Gaussians SH3, 1920x1080 spp1, cap {CAP}, 16-camera 360-degree orbit "
+                                   f"(distance 7) x {E} ensembles, one captured CUDA graph per method",
+                       "gaussians": n, "resolution": [Wt, Ht], "cameras": ncam, "ensembles_per_camera": E},
+            "methods": rows}
+    print(json.dumps(line))
+    r.close()
+    return 0
+
+
 def run_b200(args, rank, world):
     import torch
     pkg = load_package()
@@ -521,6 +573,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-micro", action="store_true", help="skip the scan/sort HBM measurements")
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoised-vs-plain PSNR measurement")
+    ap.add_argument("--config", default="default", choices=["default", "trajectory"],
+                    help="trajectory: the 2M-Gaussian 1080p 16-camera orbit through one captured graph")
+    ap.add_argument("--traj-gaussians", type=int, default=2_000_000)
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64)
     ap.add_argument("--views", default="near,mid,far", help="subset of the views (small profiling cases)")
     ap.add_argument("--ensembles", type=int, default=ENS, help="ensembles per view (small profiling cases)")
@@ -530,6 +585,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.config == "trajectory":
+        return run_trajectory(args, rank, world)
     return run_b200(args, rank, world)
 
 
