@@ -129,6 +129,7 @@ SIGNATURES = {
     "gpsb_debug_read_subpixels": (ST, [P, U32, P]),
     "gpsb_debug_error_word": (U32, [P]),
     "gpsb_load_ply": (ST, [P, SZ, P, P, P, P]),
+    "gpsb_load_ply_device": (ST, [P, SZ, P, P, P, P, P]),
     "gpsb_ply_last_error": (C.c_char_p, []),
     "gpsb_profile_enable": (ST, [P, C.c_int]),
     "gpsb_profile_read": (ST, [P, P]),

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/gpsb200.h"
+#include "ply_layout.h"
 
 namespace {
 
@@ -147,6 +148,53 @@ int find(const Header& h, const std::string& n) {
 }
 
 }  // namespace
+
+namespace gpsb {
+
+// Header, required-property lookup and SH degree of gpsb_load_ply, shared with the GPU decoder.
+gpsb_status ply_layout(const uint8_t* bytes, size_t len, PlyLayout* out) {
+    Header h;
+    gpsb_status s = parse_header(bytes, len, &h);
+    if (s != GPSB_OK) return s;
+    const char* req[] = {"x", "y", "z", "f_dc_0", "f_dc_1", "f_dc_2", "opacity", "scale_0", "scale_1", "scale_2",
+                         "rot_0", "rot_1", "rot_2", "rot_3"};
+    out->nprop = 0;
+    for (int k = 0; k < 14; ++k) {
+        int p = find(h, req[k]);
+        if (p < 0) return perr(std::string("missing required property '") + req[k] + "'");
+        out->off[out->nprop] = (uint32_t)h.props[p].off;
+        out->type[out->nprop++] = (uint8_t)h.props[p].ty;
+    }
+    int nrest = 0;
+    while (find(h, "f_rest_" + std::to_string(nrest)) >= 0) ++nrest;
+    if (nrest != 0 && nrest != 9 && nrest != 24 && nrest != 45)
+        return perr(std::to_string(nrest) + " f_rest_* properties is not 9, 24 or 45");
+    for (int r = 0; r < nrest; ++r) {
+        int p = find(h, "f_rest_" + std::to_string(r));
+        out->off[out->nprop] = (uint32_t)h.props[p].off;
+        out->type[out->nprop++] = (uint8_t)h.props[p].ty;
+    }
+    out->degree = nrest == 0 ? 0 : nrest == 9 ? 1 : nrest == 24 ? 2 : 3;
+    out->binary = h.binary;
+    out->count = h.count;
+    out->stride = h.stride;
+    out->data_start = h.data_start;
+    if (h.binary) {
+        size_t body_len = len - h.data_start;
+        if (h.stride && h.count > (size_t)-1 / h.stride) return perr("vertex count too large");
+        if (body_len < h.count * h.stride) {
+            char buf[160];
+            snprintf(buf, sizeof buf, "file truncated: need %zu bytes of vertex data, have %zu", h.count * h.stride,
+                     body_len);
+            return perr(buf);
+        }
+    }
+    return GPSB_OK;
+}
+
+gpsb_status ply_error(const char* msg) { return perr(msg); }
+
+}  // namespace gpsb
 
 extern "C" {
 

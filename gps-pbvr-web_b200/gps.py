@@ -224,6 +224,28 @@ def estimate_memory(w, h, spp_side, n):
     return {"depth_winner_bytes": a.value, "accum_bytes": b.value, "splat_bytes": c.value}
 
 
+def load_ply_device(data: bytes):
+    """GPU decode of a binary 3DGS PLY (gpsb_load_ply_device): (splats (n, 16) float32 CUDA tensor,
+    SH rest float32 CUDA tensor, degree), ready for GpsRenderer.set_gaussians_sh_device."""
+    import torch
+    L = abi.lib()
+    buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+    n = C.c_size_t()
+    d = C.c_uint32()
+    st = L.gpsb_load_ply_device(buf, len(data), C.byref(n), C.byref(d), None, None, None)
+    if st != abi.GPSB_OK:
+        raise GpsError(st, L.gpsb_ply_last_error().decode(errors="replace"))
+    per = (d.value + 1) ** 2 - 1 if d.value else 0
+    g = torch.zeros((n.value, 16), dtype=torch.float32, device="cuda")
+    sh = torch.zeros(max(n.value * 3 * per, 1), dtype=torch.float32, device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    st = L.gpsb_load_ply_device(buf, len(data), C.byref(n), C.byref(d), C.c_void_p(g.data_ptr()),
+                                C.c_void_p(sh.data_ptr()), stream)
+    if st != abi.GPSB_OK:
+        raise GpsError(st, L.gpsb_ply_last_error().decode(errors="replace"))
+    return g, sh[: n.value * 3 * per], d.value
+
+
 def load_ply(data: bytes):
     """gps-io load_ply + activation + GpuGaussian::from_activated: (splats (n,16) f32, sh_rest f32, degree)."""
     L = abi.lib()

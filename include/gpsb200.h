@@ -427,6 +427,14 @@ int gpsb_dn_crop(const void* x, const float* base, const float* target, int N, i
  * n*3*((d+1)^2-1) SH floats. */
 gpsb_status gpsb_load_ply(const uint8_t* bytes, size_t len, size_t* n_out, uint32_t* sh_degree_out,
                           gpsb_gaussian* splats, float* sh_rest);
+/* The same decode on the GPU for binary little-endian files (no counterpart in the reference,
+ * which decodes on the host): the header is parsed on the host with gpsb_load_ply's rules and
+ * messages, the vertex block is copied to the device once and decoded there one thread per
+ * vertex into splats_dev (n x 64 bytes) and sh_rest_dev (n*3*((d+1)^2-1) floats), both device
+ * memory, with the host loader's arithmetic; ready for gpsb_set_gaussians_sh_device. Two calls as
+ * for gpsb_load_ply; ASCII files are refused (GPSB_ERR_PARSE). Synchronises `cuda_stream`. */
+gpsb_status gpsb_load_ply_device(const uint8_t* bytes, size_t len, size_t* n_out, uint32_t* sh_degree_out,
+                                 gpsb_gaussian* splats_dev, float* sh_rest_dev, void* cuda_stream);
 /* Message of the last gpsb_load_ply failure on this thread (PlyError's Display, gps-io lib.rs:29-46). */
 const char* gpsb_ply_last_error(void);
 
