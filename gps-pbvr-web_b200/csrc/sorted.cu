@@ -52,7 +52,7 @@ constexpr int kMaxPasses = 8;
 #endif
 constexpr int kRsLook = GPSB_SORT_LOOKAHEAD;  // predecessor tiles read per lookback round trip
 #ifndef GPSB_SORT_BALLOT_PEERS
-#define GPSB_SORT_BALLOT_PEERS 1
+#define GPSB_SORT_BALLOT_PEERS 1  // 0 match.any, 1 ballots, 2 alternating per key
 #endif
 #ifndef GPSB_SORT_MIN_BLOCKS
 #define GPSB_SORT_MIN_BLOCKS 4
@@ -138,17 +138,21 @@ __global__ void __launch_bounds__(kRsThreads, GPSB_SORT_MIN_BLOCKS) k_onesweep(c
         bool valid = idx < n;
         key[q] = valid ? __ldg(&kin[idx]) : 0u;
         uint32_t d = valid ? ((key[q] >> shift) & (BINS - 1)) : (uint32_t)BINS;
-#if GPSB_SORT_BALLOT_PEERS
-        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+        // peer groups alternate between the ballot form (ALU pipe) and match.any (ADU pipe) so
+        // that neither pipe alone bounds the pass
+        uint32_t peers;
+        if (GPSB_SORT_BALLOT_PEERS == 1 || (GPSB_SORT_BALLOT_PEERS == 2 && (q & 1))) {
+            peers = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
-        for (int b = 0; b < BITS; ++b) {
-            uint32_t m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-            peers &= ((d >> b) & 1u) ? m : ~m;
+            for (int b = 0; b < BITS; ++b) {
+                const uint32_t bit = (d >> b) & 1u;
+                const uint32_t m = __ballot_sync(0xffffffffu, bit);
+                peers &= ~(m ^ (0u - bit));
+            }
+            if (!valid) peers = 0u;
+        } else {
+            peers = __match_any_sync(0xffffffffu, d);
         }
-        if (!valid) peers = 0u;
-#else
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
-#endif
         int leader = peers ? __ffs(peers) - 1 : lane;
         uint32_t old = 0u;
         if (valid && leader == lane) old = atomicAdd(&s_wcnt[warp][d], (uint32_t)__popc(peers));
