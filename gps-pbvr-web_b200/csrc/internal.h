@@ -24,6 +24,10 @@ struct FrameConst {
     uint32_t method, calibration, flags, sh_deg;
     float base_k, refl, object_depth;
     float jitter_sd;       // sqrt(max(low_pass, 0)), the low-pass jitter scale (gps_splat.wgsl:507)
+    // footprint-subpixel Monte-Carlo mode of the CPU oracle (GPS only; fp_fixed <= 1 and
+    // fp_kappa <= 0 = off): oracle.rs:203-235, lib.rs:412-433
+    uint32_t fp_fixed, fp_max, fp_comp;
+    float fp_kappa;
 };
 
 enum : uint32_t { FLAG_RADIAL = 1u, FLAG_CENTRE = 2u, FLAG_JITTER = 4u };

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(128) k_geometry(FrameConst f, const float4* __
         float4 r0 = make_float4(pr.mx, pr.my, pr.depth, o);
         const uint32_t method = f.method;
         const float S = (float)f.S;
-        if (method == 0u) {
+        if (method == 0u && f.fp_fixed <= 1u && !(f.fp_kappa > F_(0.0))) {
             float ex = gxc::kOffscreenSigma * sqrt_(pr.a), ey = gxc::kOffscreenSigma * sqrt_(pr.c);
             bool off = pr.mx + ex < F_(0.0) || pr.mx - ex >= (float)f.W || pr.my + ey < F_(0.0) || pr.my - ey >= (float)f.H;
             if (!off) {
@@ -59,6 +59,50 @@ __global__ void __launch_bounds__(128) k_geometry(FrameConst f, const float4* __
                 R[0] = r0;
                 R[1] = make_float4(l00, l10, l11, a);
                 R[2] = make_float4(__uint_as_float(i0), li2, F_(0.0), F_(0.0));
+            }
+        } else if (method == 0u) {
+            // footprint-subpixel mode (render_monte_carlo, oracle.rs:240-310): footprint s per splat
+            // (fixed, or adaptive from the smallest standard deviation in subpixels), the expected
+            // count divided by s^2, the sampling covariance optionally shrunk by the block's blur
+            // (s / spp_side)^2 / 12, and the off-screen skip only for s = 1
+            float det = pr.a * pr.c - pr.b * pr.b;
+            uint32_t fp = max(f.fp_fixed, 1u);
+            if (f.fp_kappa > F_(0.0)) {
+                float tr = pr.a + pr.c;
+                float disc = sqrt_(fmax_(F_(0.25) * tr * tr - det, F_(0.0)));
+                float smin = sqrt_(fmax_(F_(0.5) * tr - disc, F_(0.0))) * (float)f.side;
+                float sfp = floorf(f.fp_kappa * smin);
+                fp = !(smin > F_(0.0)) || !(sfp >= F_(1.0)) ? 1u : (sfp >= (float)f.fp_max ? f.fp_max : (uint32_t)sfp);
+            }
+            float sa = pr.a, sb = pr.b, sc = pr.c;
+            if (f.fp_comp && fp > 1u) {
+                float q = (float)fp / (float)f.side;
+                float v = q * q / F_(12.0);
+                float ta = pr.a - v, tc = pr.c - v;
+                float t = ta + tc, d = ta * tc - pr.b * pr.b;
+                if (d > F_(0.0) && t > F_(0.0) && F_(0.5) * t - sqrt_(fmax_(F_(0.25) * t * t - d, F_(0.0))) >= v) {
+                    sa = ta;
+                    sc = tc;
+                }
+            }
+            bool off = false;
+            if (fp == 1u) {
+                float ex = gxc::kOffscreenSigma * sqrt_(sa), ey = gxc::kOffscreenSigma * sqrt_(sc);
+                off = pr.mx + ex < F_(0.0) || pr.mx - ex >= (float)f.W || pr.my + ey < F_(0.0) || pr.my - ey >= (float)f.H;
+            }
+            if (!off) {
+                float li2 = dilog(o);
+                float en = f.density * S * F_(2.0) * gxc::kPi * sqrt_(det) * li2 / (float)(fp * fp);
+                if (en > F_(0.0)) cd = make_uint2(f2b(en), CD_POISSON_CAP);
+                float fo = (F_(1.0) - sqrt_(fmax_(F_(1.0) - fmin_(o, F_(1.0)), F_(0.0)))) * F_(64.0);
+                uint32_t i0 = min(f2u(fo), 63u);
+                float a = fo - (float)i0;
+                float m00 = sqrt_(fmax_(sa, F_(1e-30)));
+                float m10 = div_(sb, m00);
+                float m11 = sqrt_(fmax_(sc - m10 * m10, F_(1e-30)));
+                R[0] = r0;
+                R[1] = make_float4(m00, m10, m11, a);
+                R[2] = make_float4(__uint_as_float(i0), li2, (float)fp, F_(0.0));
             }
         } else if (method == 4u) {
             float density = fmax_(f.density, F_(1e-8));
@@ -360,6 +404,21 @@ __device__ __forceinline__ uint32_t emit_gps(const FrameConst& f, const FTabs& T
     float wx = r * cs, wy = r * sn;
     float px_ = r0.x + r1.x * wx;
     float py_ = r0.y + (r1.y * wx + r1.z * wy);
+    if (r2.z > F_(1.0)) {
+        // footprint block (write_block, oracle.rs:156-173): the s x s subpixels around the sample
+        const int s = (int)r2.z, side = (int)f.side;
+        const int gx0 = (int)floorf(px_ * (float)side - F_(0.5) * (float)s + F_(0.5));
+        const int gy0 = (int)floorf(py_ * (float)side - F_(0.5) * (float)s + F_(0.5));
+        const int gw = (int)f.W * side, gh = (int)f.H * side;
+        uint32_t wrote = 0u;
+        for (int gy = max(gy0, 0); gy < min(gy0 + s, gh); ++gy)
+            for (int gx = max(gx0, 0); gx < min(gx0 + s, gw); ++gx) {
+                const uint32_t qx = (uint32_t)(gx / side), qy = (uint32_t)(gy / side);
+                splat_write(sub, (qy * f.W + qx) * f.S + (uint32_t)(gy % side) * f.side + (uint32_t)(gx % side), r0.z, i);
+                wrote = 1u;
+            }
+        return wrote;
+    }
     if (px_ < F_(0.0) || px_ >= (float)f.W || py_ < F_(0.0) || py_ >= (float)f.H) return 0u;
     uint32_t px = f2u(px_), py = f2u(py_);
     uint32_t sx = min(f.side - 1u, f2u((px_ - (float)px) * (float)f.side));

@@ -99,6 +99,9 @@ struct gpsb_renderer {
     RadixScratch prim_sort;
     // launch-shape tuning
     uint32_t particle_items = 16, particle_blocks_per_sm = 5, ensemble_batch = 64;
+    // footprint-subpixel Monte-Carlo mode (GPS)
+    uint32_t fp_fixed = 1, fp_max = 4, fp_comp = 0;
+    float fp_kappa = 0.0f;
     // captured trajectory pipeline (gpsb_render_trajectory_graph) and the key of its work
     cudaGraphExec_t traj_exec = nullptr;
     std::vector<uint8_t> traj_key;
@@ -203,6 +206,10 @@ static FrameConst make_frame(const gpsb_renderer* r, const gpsb_camera& cam, con
     f.refl = p.pbvr.reference_pixel_length;
     double d[3] = {r->centroid[0] - cam.view_pos[0], r->centroid[1] - cam.view_pos[1], r->centroid[2] - cam.view_pos[2]};
     f.object_depth = (float)(R[6] * d[0] + R[7] * d[1] + R[8] * d[2]);
+    f.fp_fixed = r->fp_fixed;
+    f.fp_max = r->fp_max;
+    f.fp_comp = r->fp_comp;
+    f.fp_kappa = r->fp_kappa;
     return f;
 }
 
@@ -471,6 +478,18 @@ void gpsb_destroy(gpsb_renderer* r) {
     if (r->stats_event) cudaEventDestroy(r->stats_event);
     if (r->own) cudaStreamDestroy(r->own);
     delete r;
+}
+
+gpsb_status gpsb_set_footprint(gpsb_renderer* r, uint32_t footprint_subpixels, float adaptive_kappa,
+                              uint32_t footprint_max, uint32_t compensate_blur) {
+    if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
+    if (footprint_subpixels > 64 || footprint_max > 64 || !(adaptive_kappa >= 0.0f) || !isfinite(adaptive_kappa))
+        return fail(r, GPSB_ERR_INVALID_ARGUMENT, "footprint sizes must be 0..64 and kappa finite and >= 0");
+    r->fp_fixed = std::max(footprint_subpixels, 1u);
+    r->fp_max = std::max(footprint_max, 1u);
+    r->fp_comp = compensate_blur ? 1u : 0u;
+    r->fp_kappa = adaptive_kappa;
+    return GPSB_OK;
 }
 
 gpsb_status gpsb_set_feature_accum(gpsb_renderer* r, float* feat_dev) {

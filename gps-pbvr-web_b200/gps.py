@@ -437,6 +437,11 @@ class GpsRenderer:
         self._ck(self._L.gpsb_debug_read_subpixels(self._r, slot, out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def set_footprint(self, footprint_subpixels=1, adaptive_kappa=0.0, footprint_max=4, compensate_blur=False):
+        """Footprint-subpixel Monte-Carlo mode of GPS (MonteCarloOptions of the CPU oracle)."""
+        self._ck(self._L.gpsb_set_footprint(self._r, footprint_subpixels, adaptive_kappa, footprint_max,
+                                            int(bool(compensate_blur))))
+
     def set_feature_accum(self, feat):
         """Denoiser feature sums into `feat` (a zeroed CUDA tensor of W*H*8 float32), or None to stop."""
         self._ck(self._L.gpsb_set_feature_accum(self._r, C.c_void_p(feat.data_ptr()) if feat is not None else None))

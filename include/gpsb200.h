@@ -169,6 +169,15 @@ gpsb_status gpsb_create(int device, uint32_t width, uint32_t height, uint32_t sp
 void gpsb_destroy(gpsb_renderer* r);
 /* Run the renderer's work on an external cudaStream_t (NULL restores its own stream). */
 gpsb_status gpsb_set_stream(gpsb_renderer* r, void* cuda_stream);
+/* Footprint-subpixel Monte-Carlo mode of the GPS method (the reference has it only in its CPU
+ * oracle: render_monte_carlo's MonteCarloOptions, crates/gps-core/src/oracle.rs:203-310,
+ * lib.rs:412-433): each particle writes a footprint_subpixels x footprint_subpixels block of
+ * subpixels (write_block) and the expected count is divided by its area; adaptive_kappa > 0
+ * picks the footprint per splat as floor(kappa * smallest standard deviation in subpixels),
+ * clamped to 1..footprint_max; compensate_blur shrinks the sampling covariance by the block's
+ * blur. footprint_subpixels <= 1 with adaptive_kappa = 0 is the normal GPS renderer. */
+gpsb_status gpsb_set_footprint(gpsb_renderer* r, uint32_t footprint_subpixels, float adaptive_kappa,
+                              uint32_t footprint_max, uint32_t compensate_blur);
 /* Denoiser features (no counterpart in the reference, which has no denoiser): with feat_dev set
  * (device memory of the caller, width*height*8 floats, zeroed by the caller), every rendered
  * ensemble also adds, per pixel, (r^2, g^2, b^2, alpha, depth) of its resolved colour, covered

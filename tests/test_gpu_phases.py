@@ -295,3 +295,30 @@ def test_tuning_does_not_change_results(tune):
         b, sb = gpu_mean(items, p, 10, renderer=r)
         r.close()
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)) and sa.counters() == sb.counters()
+
+
+@pytest.mark.parametrize("kw", [{"footprint_subpixels": 2, "compensate_blur": True},
+                                {"footprint_subpixels": 3},
+                                {"adaptive_kappa": 0.6, "footprint_max": 4, "compensate_blur": True}],
+                         ids=["fixed2_blur", "fixed3", "adaptive"])
+def test_footprint_mode_vs_oracle(kw):
+    """The footprint-subpixel Monte-Carlo mode on the GPU against the oracle's render_monte_carlo
+    with the same options and the GPU's per-particle seeds (oracle.rs:203-310): PSNR >= 60 dB and
+    the same Poisson point counts within 4 sigma, as for plain GPS."""
+    from _scenes import layers
+    items = layers()
+    r = PKG.GpsRenderer(W, H, SIDE)
+    r.set_footprint(footprint_subpixels=kw.get("footprint_subpixels", 1), adaptive_kappa=kw.get("adaptive_kappa", 0.0),
+                    footprint_max=kw.get("footprint_max", 4), compensate_blur=kw.get("compensate_blur", False))
+    p = params()
+    acc, st = gpu_mean(items, p, SETS, renderer=r)
+    r.close()
+    cpu, cst = O.render_monte_carlo(scene(items), cam17(), W, H, SIDE, SETS, BG, 1, per_particle_seed=True,
+                                    max_points_per_splat=p.max_points_per_splat, threads=8, **kw)
+    gpu = image(acc)
+    tol = 4.0 * max(math.sqrt(2.0 * cst["points"]), 1.0)
+    assert O.psnr(gpu, cpu) >= 60.0, O.psnr(gpu, cpu)
+    assert abs(st.points - cst["points"]) <= tol
+    # the footprint really changes the image statistics: fewer points than plain GPS
+    plain_acc, plain_st = gpu_mean(items, p, SETS)
+    assert st.points < plain_st.points
