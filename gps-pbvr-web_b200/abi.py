@@ -100,6 +100,9 @@ SIGNATURES = {
     "gpsb_set_stream": (ST, [P, P]),
     "gpsb_set_feature_accum": (ST, [P, P]),
     "gpsb_set_footprint": (ST, [P, U32, C.c_float, U32, U32]),
+    "gpsb_set_fast_decisions": (ST, [P, U32]),
+    "gpsb_debug_fast_counts": (ST, [P, P]),
+    "gpsb_debug_fast_bounds": (ST, [P, P]),
     "gpsb_set_gaussians": (ST, [P, P, SZ]),
     "gpsb_set_gaussians_sh": (ST, [P, P, SZ, P, SZ, U32]),
     "gpsb_set_gaussians_sh_device": (ST, [P, P, SZ, P, SZ, U32]),

@@ -28,6 +28,7 @@ struct FrameConst {
     // fp_kappa <= 0 = off): oracle.rs:203-235, lib.rs:412-433
     uint32_t fp_fixed, fp_max, fp_comp;
     float fp_kappa;
+    uint32_t fast_mode;  // PBVR fast decisions: 0 off, 1 on, 2 validate (exact always, count disagreements)
 };
 
 enum : uint32_t { FLAG_RADIAL = 1u, FLAG_CENTRE = 2u, FLAG_JITTER = 4u };
@@ -51,7 +52,7 @@ constexpr int kRecF4 = 6;
 enum : int {
     ST_POINTS = 0, ST_TRUNCATED = 1, ST_DROPPED = 2, ST_VISIBLE = 3, ST_ORPHAN = 4, ST_CANDIDATES = 5,
     ST_UNDERCOVERED = 6, ST_SKIPPED = 7, ST_ENSEMBLES = 8, ST_PROBE = 9, ST_WRITES = 10, ST_ENTRIES = 11,
-    ST_WORDS = 16
+    ST_FAST_EXACT = 12, ST_FAST_MISMATCH = 13, ST_WORDS = 16
 };
 
 // Device error word bits (bounded waits that gave up).
@@ -83,6 +84,7 @@ void launch_geometry(const FrameConst& fc, const float4* splats, const float* sh
 void launch_count_scan(const FrameConst& fc, const uint2* cdesc, uint32_t first_seed, uint32_t E, uint64_t* lookback,
                        uint32_t* tile_counter, uint2* clist, EnsTotal* etot, unsigned long long* stats,
                        uint32_t* err, cudaStream_t st);
+void launch_fast_bounds(uint32_t* out, cudaStream_t st);
 void launch_particles(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
                       const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
                       uint32_t* unit_counter, unsigned long long* stats, int grid, int items, cudaStream_t st);

@@ -13,6 +13,9 @@
 #include "devmath.cuh"
 
 // Resident blocks per SM the particle kernel is compiled for (register budget).
+#ifndef GPSB_FAST_MIN_BLOCKS
+#define GPSB_FAST_MIN_BLOCKS 4  // resident blocks per SM of the PBVR fast-decision variant
+#endif
 #ifndef GPSB_PARTICLE_MIN_BLOCKS
 #define GPSB_PARTICLE_MIN_BLOCKS 5
 #endif
@@ -20,6 +23,77 @@
 namespace gpsb {
 
 typedef unsigned long long ull;
+
+// ---------------------------------------------------------------- fast decisions (PBVR)
+// Most particles of a close view are never written: in the near orbit of a 560k-splat scene at
+// 1280x720, 98.6 % of them fall off screen, behind the near plane or out of the radial keep test,
+// and all that matters for them is whether they count as points. pbvr_fast answers that with the
+// MUFU approximations (lg2 / rsqrt / sin / cos / ex2 / rcp, flush-to-zero forms) and bounds on
+// |fast value - exact f32 value|; whenever a bound straddles a threshold, or the particle may
+// land on screen, it answers 2 and the caller runs the exact path (emit_pbvr) from the
+// particle's own stream. Its answers are therefore the exact path's:
+//   0 = not a point, 1 = a point off screen (no write), 2 = undecided (run emit_pbvr).
+// Error model: every standard normal the fast path draws is within kEN of the exact path's and
+// at most kRMax in size (pairs with x = -2 log u1 < kXMin are left undecided), so the camera
+// coordinates' bounds are per-splat constants, written by the geometry kernel into unused lanes
+// of the record (fast_bounds_of); from there on, each step adds its propagated error, 2 kU per
+// rounding of either path times the magnitude rounded, and kSafe for the rounding of the bound
+// arithmetic itself. The constants of the approximations are checked against the exact maths
+// over every input they can get (gpsb_debug_fast_bounds); the exact maths' own errors are those
+// of fmath.h (exp 2 ulp, log 4 * 2^-24 relative or 2e-7 absolute).
+constexpr float kU = 6.0e-8f, kSafe = 1.01f;
+constexpr float kLogAbs = 7e-7f, kLogRel = 7e-7f;   // |mlog(v) - log(v)| <= kLogAbs + kLogRel |mlog(v)|, v in [kUMin, 1)
+constexpr float kSinCos = 2e-6f;                    // |msin/mcos(t) - sincos(t)|, t = RN(2 pi u), u = k 2^-24
+constexpr float kXMin = 1e-3f;                      // smallest x = -2 log u1 the bounds cover
+constexpr float kErMax = 4.6e-5f;                   // |r - r_exact| for x >= kXMin (r = x rsqrt(x))
+constexpr float kRMax = 5.77f;                      // largest r (u1 >= kUMin)
+constexpr float kEN = kErMax * (1.0f + 2.0f * kSinCos) + kRMax * (kSinCos + 2.01f * kU) + 1e-7f;  // one normal
+constexpr float kExpA = 6e-7f, kExpB = 1.5e-7f;     // |mexp(a) - exp(a)| <= (kExpA + kExpB |a|) mexp(a) + kExpTiny, a <= 0
+constexpr float kExpTiny = 1.5e-38f;
+constexpr float kLn2 = 0.693147182f, kLog2e = 1.44269502f;
+
+__device__ __forceinline__ float mufu(float x, int op) {
+    float y;
+    switch (op) {
+        case 0: asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); break;
+        case 1: asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); break;
+        case 2: asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); break;
+        case 3: asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); break;
+        case 4: asm("sin.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); break;
+        default: asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); break;
+    }
+    return y;
+}
+__device__ __forceinline__ float mlog(float x) { return mufu(x, 0) * kLn2; }
+__device__ __forceinline__ float mexp(float a) { return mufu(a * kLog2e, 1); }
+
+// Per-splat bounds of the fast path's camera coordinates (written by the geometry kernel into
+// r1.z = |fx| ecx, r1.w = |fy| ecy, r3.z = ecz, r3.w = |a| + 2|b| + |c|, r4.w = 2(|a| + |b|),
+// r5.w = 2(|b| + |c|) for the conic (a, b, c) = (r2.w, r3.x, r3.y)). World w_j = centre_j +
+// sum_k L_jk u_k (2, 4, 6 operations), p = w - camera (one more), c_i = dot3(rot_i, p) (5 more).
+__device__ __forceinline__ void fast_bounds_of(const FrameConst& f, float3 g0, float k00, float k10, float k11,
+                                               float k20, float k21, float k22, float a, float b, float c,
+                                               float4& r1, float4& r3, float4& r4, float4& r5) {
+    const float sx = fabsf(k00), sy = fabsf(k10) + fabsf(k11), sz = fabsf(k20) + fabsf(k21) + fabsf(k22);
+    const float gm = kRMax + kEN;
+    const float Mx = fabsf(g0.x) + fabsf(f.pos[0]) + sx * gm, My = fabsf(g0.y) + fabsf(f.pos[1]) + sy * gm,
+                Mz = fabsf(g0.z) + fabsf(f.pos[2]) + sz * gm;
+    const float ex = sx * kEN + F_(6.0) * kU * Mx, ey = sy * kEN + F_(10.0) * kU * My, ez = sz * kEN + F_(14.0) * kU * Mz;
+    auto row = [&](const float* q) {
+        const float ax = fabsf(q[0]), ay = fabsf(q[1]), az = fabsf(q[2]);
+        return (ax * ex + ay * ey + az * ez + F_(10.0) * kU * (ax * (Mx + ex) + ay * (My + ey) + az * (Mz + ez))) * F_(1.02);
+    };
+    const float ecx = row(f.rot0), ecy = row(f.rot1), ecz = row(f.rot2);
+    r1.z = fabsf(f.fx) * ecx * F_(1.02);
+    r1.w = fabsf(f.fy) * ecy * F_(1.02);
+    r3.z = ecz;
+    r3.w = (fabsf(a) + F_(2.0) * fabsf(b) + fabsf(c)) * F_(1.02);
+    r4.w = F_(2.0) * (fabsf(a) + fabsf(b)) * F_(1.02);
+    r5.w = F_(2.0) * (fabsf(b) + fabsf(c)) * F_(1.02);
+    if (!isfinite(ecx) || !isfinite(ecy) || !isfinite(ecz) || !isfinite(r3.w)) {
+        r1.z = r1.w = r3.z = r3.w = r4.w = r5.w = __int_as_float(0x7F800000);  // never decides
+    }
+}
 
 // ============================================================================ geometry
 // Once per camera: projection, opacity clamp, per-method count descriptor and particle record,
@@ -168,12 +242,18 @@ __global__ void __launch_bounds__(128) k_geometry(FrameConst f, const float4* __
                 float k11 = sqrt_(fmax_(a11 - k10 * k10, F_(1e-30)));
                 float k21 = div_(a21 - k20 * k10, k11);
                 float k22 = sqrt_(fmax_(a22 - k20 * k20 - k21 * k21, F_(1e-30)));
+                float4 q1 = make_float4(keep, eol(fmin_(o, gxc::kOneMinus1e6)), F_(0.0), F_(0.0));
+                float4 q3 = make_float4(-pr.b * idet, pr.a * idet, F_(0.0), F_(0.0));
+                float4 q4 = make_float4(k00, k10, k11, F_(0.0));
+                float4 q5 = make_float4(k20, k21, k22, F_(0.0));
+                fast_bounds_of(f, make_float3(g0.x, g0.y, g0.z), k00, k10, k11, k20, k21, k22, pr.c * idet, q3.x, q3.y,
+                               q1, q3, q4, q5);
                 R[0] = r0;
-                R[1] = make_float4(keep, eol(fmin_(o, gxc::kOneMinus1e6)), F_(0.0), F_(0.0));
+                R[1] = q1;
                 R[2] = make_float4(g0.x, g0.y, g0.z, pr.c * idet);
-                R[3] = make_float4(-pr.b * idet, pr.a * idet, F_(0.0), F_(0.0));
-                R[4] = make_float4(k00, k10, k11, F_(0.0));
-                R[5] = make_float4(k20, k21, k22, F_(0.0));
+                R[3] = q3;
+                R[4] = q4;
+                R[5] = q5;
             }
         }
     }
@@ -494,6 +574,164 @@ __device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, const FTabs& 
     return 3u;
 }
 
+// One Box-Muller pair from the stream, drawn in the order of Normal::next (cos part, sin part).
+// Returns false when x = -2 log u1 is below kXMin, where the kEN bound does not hold.
+__device__ __forceinline__ bool fast_pair(uint32_t& st, float& c, float& s) {
+    const float u1 = fmax_(gx::next_u(&st), gxc::kUMin);
+    const float u2 = gx::next_u(&st);
+    const float x = -F_(2.0) * mlog(u1);
+    const float r = x * mufu(x, 2);
+    const float t = gxc::kTwoPi * u2;
+    c = r * mufu(t, 5);
+    s = r * mufu(t, 4);
+    return x >= kXMin;
+}
+
+// Straight-line form: every lane computes the whole path and the answer is selected at the end
+// (the lanes of a warp rarely agree on an early exit, and divergent exits cost more than they save).
+__device__ __forceinline__ uint32_t pbvr_fast(const FrameConst& f, uint32_t st, const float4* R) {
+    float uz, uy, ux, jy;
+    bool ok = fast_pair(st, uz, uy);
+    ok &= fast_pair(st, ux, jy);  // jy is the pair's spare, used by the jitter
+    const float4 r1 = R[1];
+    if (f.method == 3u) {
+        if (gx::next_u(&st) >= r1.x) return 0u;  // the exact draw and test
+    }
+    const float4 r2 = R[2], r3 = R[3], r4 = R[4], r5 = R[5];
+    const float px = __fmaf_rn(r4.x, ux, r2.x) - f.pos[0];
+    const float py = __fmaf_rn(r4.z, uy, __fmaf_rn(r4.y, ux, r2.y)) - f.pos[1];
+    const float pz = __fmaf_rn(r5.z, uz, __fmaf_rn(r5.y, uy, __fmaf_rn(r5.x, ux, r2.z))) - f.pos[2];
+    const float cz = __fmaf_rn(f.rot2[2], pz, __fmaf_rn(f.rot2[1], py, f.rot2[0] * px));
+    const float ecz = r3.z * kSafe;
+    const bool behind = cz + ecz <= f.near_z;  // surely not a point
+    const float czl = cz - ecz;
+    bool sure = czl > f.near_z && czl > F_(3.0) * ecz && cz < 1e30f && czl > 1e-6f;  // surely in front
+    const float cx = __fmaf_rn(f.rot0[2], pz, __fmaf_rn(f.rot0[1], py, f.rot0[0] * px));
+    const float cy = __fmaf_rn(f.rot1[2], pz, __fmaf_rn(f.rot1[1], py, f.rot1[0] * px));
+    // t = (f c) / cz; |t - t'| <= (|f| ec + |t| ecz) / (cz - ecz) + the reciprocal's and both
+    // paths' roundings (1e-6 |t|), 1 / (cz - ecz) <= (1 + 2 ecz / cz) / cz for ecz <= cz / 4;
+    // then + f.cx with one more rounding in each path
+    const float icz = mufu(cz, 3);
+    const float icl = icz * __fmaf_rn(F_(2.0) * ecz, icz, F_(1.0)) * kSafe;
+    const float kt = __fmaf_rn(ecz, icl, 1e-6f + F_(2.0) * kU);
+    const float tx = (f.fx * cx) * icz, ty = (f.fy * cy) * icz;
+    float pix_x = tx + f.cx, pix_y = ty + f.cy;
+    float epx = __fmaf_rn(fabsf(tx), kt, __fmaf_rn(r1.z, icl, F_(2.0) * kU * fabsf(f.cx)));
+    float epy = __fmaf_rn(fabsf(ty), kt, __fmaf_rn(r1.w, icl, F_(2.0) * kU * fabsf(f.cy)));
+    const uint32_t flags = f.flags;
+    if (flags & FLAG_JITTER) {
+        float jx, js;
+        sure &= fast_pair(st, jx, js);
+        // |sd j - sd j'| <= |sd| kEN, + the product's and the sum's roundings in both paths
+        const float kj = fabsf(f.jitter_sd) * (kEN + F_(4.0) * kU * kRMax);
+        pix_x = pix_x + f.jitter_sd * jx;
+        pix_y = pix_y + f.jitter_sd * jy;
+        epx = __fmaf_rn(F_(4.0) * kU, fabsf(pix_x), epx + kj);
+        epy = __fmaf_rn(F_(4.0) * kU, fabsf(pix_y), epy + kj);
+    }
+    sure &= fabsf(pix_x) < 1e30f && fabsf(pix_y) < 1e30f && epx < 1e30f && epy < 1e30f;
+    const float mx = kSafe * epx, my = kSafe * epy;
+    const bool off = pix_x + mx < F_(0.0) || pix_x - mx >= (float)f.W || pix_y + my < F_(0.0) || pix_y - my >= (float)f.H;
+    uint32_t res = off ? 1u : 2u;
+    if (flags & FLAG_RADIAL) {
+        const float4 r0 = R[0];
+        const float dvx = pix_x - r0.x, dvy = pix_y - r0.y;
+        const float e = fmaxf(__fmaf_rn(F_(2.0) * kU, fabsf(pix_x) + fabsf(r0.x), epx),
+                              __fmaf_rn(F_(2.0) * kU, fabsf(pix_y) + fabsf(r0.y), epy));
+        // r2v = a dx^2 + 2 b dx dy + c dy^2: |grad . d| <= e (G_x |dx| + G_y |dy|), |Q(d)| <= K e^2,
+        // roundings <= 20 kU (|a| + |b|) dx^2 + (|b| + |c|) dy^2
+        const float dx2 = dvx * dvx, dy2 = dvy * dvy;
+        const float r2v = __fmaf_rn(r2.w, dx2, __fmaf_rn(F_(2.0) * r3.x, dvx * dvy, r3.y * dy2));
+        const float m2 = __fmaf_rn(r4.w, dx2, r5.w * dy2);
+        const float er2 = __fmaf_rn(__fmaf_rn(r4.w, fabsf(dvx), r5.w * fabsf(dvy)), e, __fmaf_rn(r3.w * e, e, F_(10.0) * kU * m2));
+        const float arg = -F_(0.5) * fmaxf(r2v, F_(0.0));
+        const float earg = F_(0.5) * er2 * kSafe;
+        // y = min(o, 1 - 1e-6) exp(arg): propagated error (e^earg - 1 <= earg (1 + earg)), the
+        // approximation against exp, exp's own 2 ulp at both arguments, the product's roundings;
+        // with earg < 1/8 every relative term grows by at most (1 + 2 earg) <= 1.25
+        const float oo = fmin_(r0.w, gxc::kOneMinus1e6);
+        const float y = oo * mexp(arg);
+        const float rel = __fmaf_rn(earg, F_(1.0) + earg, __fmaf_rn(kExpB, fabsf(arg), kExpA + F_(5.4e-7) + F_(2.0) * kU));
+        const float ey = __fmaf_rn(y, rel * (F_(1.25) * kSafe), F_(2.02) * kExpTiny);
+        // eol's short form (both paths take it when y + ey < 1e-4) ...
+        const bool small = y + ey < F_(1e-4);
+        const float eo_s = F_(1.0) + F_(0.5) * y;
+        const float eeo_s = __fmaf_rn(F_(0.5), ey, F_(2.0) * kU * eo_s);
+        // ... and its log form, eol(y) = -log(1 - y) / y, with 1 / (a - e) <= (1 + 2 e / a) / a for
+        // e <= a / 2: the approximation against log at v, log's own error at both arguments,
+        // the argument's error
+        const float v = F_(1.0) - fmin_(y, gxc::kOneMinus1e6);
+        const float ev = ey + F_(2.0) * kU;
+        const float lg = mlog(v);
+        const float iv = mufu(v, 3), iy = mufu(y, 3);
+        const float elg = __fmaf_rn(kLogRel + F_(5e-7), fabsf(lg), kLogAbs + F_(4e-7)) +
+                          ev * iv * __fmaf_rn(F_(2.0) * ev, iv, F_(1.0)) * kSafe;
+        const float eo_l = -lg * iy;
+        const float eeo_l = __fmaf_rn(__fmaf_rn(fabsf(eo_l), ey, elg) * iy, __fmaf_rn(F_(2.0) * ey, iy, F_(1.0)) * kSafe,
+                                      F_(4e-7) * fabsf(eo_l));
+        const bool large = y - ey >= F_(1e-4) && ev <= F_(0.5) * v && ey <= F_(0.5) * y;
+        sure &= earg < F_(0.125) && (small || large);
+        const float eo = small ? eo_s : eo_l, de = (small ? eeo_s : eeo_l) * kSafe;
+        // keep = clamp(eo / r1.y, 0, 1) against the exact draw, compared as u r1.y against eo
+        const float ur = gx::next_u(&st) * r1.y;
+        const bool reject = ur >= (eo + de) * (F_(1.0) + F_(6.0) * kU);
+        const bool keep = ur * (F_(1.0) + F_(6.0) * kU) < eo - de;
+        res = reject ? 0u : (keep ? res : 2u);
+    }
+    res = behind ? 0u : (sure ? res : 2u);
+    return ok ? res : 2u;
+}
+
+// Exhaustive check of the constants of the fast decisions: the largest |approximation - exact| /
+// bound over every input the approximations get, out[0..5] as float bits (ratios <= 1 hold the
+// bounds): log over the uniforms k 2^-24; log over every float in [1e-6, 1); sin and cos over
+// 2 pi k 2^-24; |r - r_exact| / kErMax over the uniforms with x >= kXMin; r / kRMax; exp over
+// every float in [-128, 0]. NaN shows as infinity.
+__device__ __forceinline__ void upd_ratio(float& m, float v) { m = v != v ? __int_as_float(0x7F800000) : fmaxf(m, v); }
+
+__global__ void __launch_bounds__(256) k_fast_bounds(uint32_t* out) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    float m[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (uint32_t k = tid; k < (1u << 24); k += nth) {
+        const float u = (float)k * (1.0f / 16777216.0f);
+        const float u1 = fmax_(u, gxc::kUMin);
+        const float L = mlog(u1), Le = gx::log(u1);
+        upd_ratio(m[0], fabsf(L - Le) / __fmaf_rn(kLogRel, fabsf(L), kLogAbs));
+        // r exactly as fast_pair and Normal::next compute it
+        const float x = -F_(2.0) * L;
+        const float r = x * mufu(x, 2);
+        const float re = sqrt_(-F_(2.0) * Le);
+        if (x >= kXMin) {
+            upd_ratio(m[3], fabsf(r - re) / kErMax);
+            upd_ratio(m[4], r / kRMax);
+        }
+        const float t = gxc::kTwoPi * u;
+        float se, ce;
+        gx::sincos(t, &se, &ce);
+        upd_ratio(m[2], fmaxf(fabsf(mufu(t, 4) - se), fabsf(mufu(t, 5) - ce)) / kSinCos);
+    }
+    for (uint32_t b = __float_as_uint(1e-6f) + tid; b < 0x3F800000u; b += nth) {
+        const float v = __uint_as_float(b);
+        const float L = mlog(v);
+        upd_ratio(m[1], fabsf(L - gx::log(v)) / __fmaf_rn(kLogRel, fabsf(L), kLogAbs));
+    }
+    for (uint32_t b = 0x80000000u + tid; b <= 0xC3000000u; b += nth) {
+        const float a = __uint_as_float(b);
+        const float y = mexp(a);
+        upd_ratio(m[5], fabsf(y - gx::exp(a)) / __fmaf_rn(__fmaf_rn(kExpB, fabsf(a), kExpA), y, kExpTiny));
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        const uint32_t w = __reduce_max_sync(0xffffffffu, __float_as_uint(m[c]));
+        if ((threadIdx.x & 31) == 0 && w) atomicMax(&out[c], w);
+    }
+}
+
+void launch_fast_bounds(uint32_t* out, cudaStream_t st) {
+    cudaMemsetAsync(out, 0, 6 * sizeof(uint32_t), st);
+    k_fast_bounds<<<148 * 8, 256, 0, st>>>(out);
+}
+
 // ScreenOccupancy branch of particle_pass (gps_splat.wgsl:686-708); returns 1 on a hit
 __device__ __forceinline__ uint32_t emit_so(const FrameConst& f, const FTabs& T, uint32_t i, uint32_t k, uint32_t& rs,
                                             const float4* R, ull* sub) {
@@ -522,6 +760,9 @@ __device__ __forceinline__ uint32_t emit_so(const FrameConst& f, const FTabs& T,
 }
 
 constexpr int kPT = 256;               // threads per particle block
+constexpr uint32_t kRing = 64;         // per-warp ring of undecided PBVR particles (uint2 entries)
+constexpr uint32_t kFastGiveUp = 10;   // undecided lanes of one step above which a warp stops the fast test
+static_assert(kTabFloats % 2 == 0, "the ring after the entry lists needs 8-byte alignment");
 
 // Largest j in [lo, hi) with off(j) <= v, by a 32-ary warp search (off(lo) <= v must hold).
 __device__ __forceinline__ uint32_t warp_last_le(const uint2* __restrict__ L, uint32_t lo, uint32_t hi, uint64_t v, int lane) {
@@ -544,14 +785,16 @@ __device__ __forceinline__ uint32_t warp_last_le(const uint2* __restrict__ L, ui
 // the compact list, regenerates it from its own stream particle_seed(i, k + 1, seed) and writes it
 // with one 64-bit atomicMin of (depth key << 32 | i), which equals the reference's depth pass
 // followed by the colour pass (gps_splat.wgsl:276-281). Ensembles flagged skipped get no work.
-template <int MC, int kPIPT>  // MC: 0 GPS, 1 PBVR, 2 ScreenOccupancy; kPIPT: particles per thread per tile
-__global__ void __launch_bounds__(kPT, GPSB_PARTICLE_MIN_BLOCKS) k_particles(FrameConst f, const float4* __restrict__ rec,
+// MC: 0 GPS, 1 PBVR, 2 ScreenOccupancy; kPIPT: particles per thread per tile; FM: PBVR fast decisions
+// (0 off, 1 on, 2 validate), a template parameter so each variant gets its own register allocation
+template <int MC, int kPIPT, int FM>
+__global__ void __launch_bounds__(kPT, FM == 1 ? GPSB_FAST_MIN_BLOCKS : GPSB_PARTICLE_MIN_BLOCKS) k_particles(FrameConst f, const float4* __restrict__ rec,
                                                    const float* __restrict__ lut, const uint2* __restrict__ clist,
                                                    const EnsTotal* __restrict__ etot, uint32_t first_seed, uint32_t E,
                                                    ull* sub, uint32_t* unit_counter, ull* stats) {
     constexpr int kPTile = kPT * kPIPT;  // particles per tile
     // dynamic shared memory: [fmath tables (kTabFloats)] [first unit of each ensemble (E + 1)]
-    // [entry offsets (kPTile + 2)] [entry ids (kPTile + 2)] [radius table (GPS)]
+    // [entry offsets (kPTile + 2)] [entry ids (kPTile + 2)] [radius table (GPS) | rings (PBVR fast)]
     extern __shared__ __align__(16) uint32_t s_dyn[];
     const FTabs T = stage_tabs(reinterpret_cast<float*>(s_dyn));
     uint64_t* s_ubase = reinterpret_cast<uint64_t*>(s_dyn + kTabFloats);
@@ -575,7 +818,7 @@ __global__ void __launch_bounds__(kPT, GPSB_PARTICLE_MIN_BLOCKS) k_particles(Fra
     __syncthreads();
     const uint64_t total_units = s_ubase[E];
     const uint64_t PS = (uint64_t)f.W * f.H * f.S;
-    uint32_t points = 0, writes = 0;
+    uint32_t points = 0, writes = 0, exact_runs = 0, mismatch = 0;
     for (;;) {
         if (tid == 0) s_unit = atomicAdd(unit_counter, 1u);
         __syncthreads();
@@ -613,7 +856,87 @@ __global__ void __launch_bounds__(kPT, GPSB_PARTICLE_MIN_BLOCKS) k_particles(Fra
         const uint32_t seed = first_seed + e;
         ull* S = sub + (size_t)e * PS;
         uint64_t p = p0 + (uint64_t)tid * kPIPT;
-        if (p < p1) {
+        if (MC == 1 && FM == 1) {
+            // Converged warp loop over the fast decisions: the particles pbvr_fast leaves undecided
+            // go to a per-warp ring in shared memory and run the exact path 32 at a time with the
+            // whole warp, instead of once for every divergent lane. A warp whose lanes are mostly
+            // undecided (on-screen work) drops the fast test for the rest of the tile.
+            uint2* ring = reinterpret_cast<uint2*>(s_lut) + (size_t)(tid >> 5) * kRing;
+            const uint32_t below = (1u << lane) - 1u;
+            uint32_t head = 0u, count = 0u, pp = 0u, pend = 0u, jj = 0u, cur = 0xFFFFFFFFu;
+            bool fast = true;
+            float4 R[kRecF4];
+            if (p < p1) {
+                pp = (uint32_t)p;
+                uint32_t a = 0, b = w;
+                while (b - a > 1u) {
+                    uint32_t m = (a + b) >> 1;
+                    if (s_off[m] <= pp) a = m; else b = m;
+                }
+                jj = a;
+                pend = (uint32_t)(p + kPIPT < p1 ? p + kPIPT : p1);
+            }
+            auto load_rec = [&](uint32_t i) {
+                const float4* Rg = rec + (size_t)i * kRecF4;
+#pragma unroll
+                for (int c = 0; c < kRecF4; ++c) R[c] = __ldg(&Rg[c]);
+                cur = i;
+            };
+            auto run_exact = [&](uint32_t i, uint32_t k) {
+                if (i != cur) load_rec(i);
+                uint32_t rs = gx::particle_seed(i, k + 1u, seed);
+                const uint32_t r = emit_pbvr(f, T, i, rs, R, S);
+                points += r & 1u;
+                writes += r >> 1;
+            };
+            uint32_t nxt = 0u, ci = 0u, ck = 0u;  // next entry boundary, current splat and index
+            if (pp < pend) {
+                ci = s_id[jj];
+                ck = pp - s_off[jj];
+                nxt = s_off[jj + 1];
+            }
+            for (int it = 0; it < kPIPT; ++it) {
+                uint32_t need = 0u, i = 0u, k = 0u;
+                if (pp < pend) {
+                    if (pp >= nxt) {
+                        while (pp >= s_off[jj + 1]) ++jj;
+                        ci = s_id[jj];
+                        ck = pp - s_off[jj];
+                        nxt = s_off[jj + 1];
+                    }
+                    i = ci;
+                    k = ck++;
+                    ++pp;
+                    if (fast) {
+                        if (i != cur) load_rec(i);
+                        const uint32_t q = pbvr_fast(f, gx::particle_seed(i, k + 1u, seed), R);
+                        if (q == 2u) need = 1u; else points += q;
+                    } else {
+                        run_exact(i, k);
+                    }
+                }
+                const uint32_t bal = __ballot_sync(0xffffffffu, need);
+                if (bal == 0u) continue;
+                const uint32_t n = (uint32_t)__popc(bal);
+                if (need) ring[(head + count + (uint32_t)__popc(bal & below)) & (kRing - 1u)] = make_uint2(i, k);
+                count += n;
+                exact_runs += need;
+                if (n > kFastGiveUp) fast = false;
+                if (count >= 32u) {
+                    __syncwarp();
+                    const uint2 q = ring[(head + (uint32_t)lane) & (kRing - 1u)];
+                    __syncwarp();
+                    head += 32u;
+                    count -= 32u;
+                    run_exact(q.x, q.y);
+                }
+            }
+            __syncwarp();
+            if ((uint32_t)lane < count) {
+                const uint2 q = ring[(head + (uint32_t)lane) & (kRing - 1u)];
+                run_exact(q.x, q.y);
+            }
+        } else if (p < p1) {
             uint32_t pp = (uint32_t)p;
             // entry of particle pp in the window
             uint32_t a = 0, b = w;
@@ -647,7 +970,19 @@ __global__ void __launch_bounds__(kPT, GPSB_PARTICLE_MIN_BLOCKS) k_particles(Fra
                 if (MC == 0) {
                     writes += emit_gps(f, T, s_lut, i, rs, R[0], R[1], R[2], S);
                 } else if (MC == 1) {
-                    uint32_t r = emit_pbvr(f, T, i, rs, R, S);
+                    uint32_t r;
+                    if (FM == 0) {
+                        r = emit_pbvr(f, T, i, rs, R, S);
+                    } else {
+                        const uint32_t q = pbvr_fast(f, rs, R);
+                        if (FM == 2) {  // validation: always exact, count disagreements
+                            r = emit_pbvr(f, T, i, rs, R, S);
+                            mismatch += (q != 2u && q != r) ? 1u : 0u;
+                        } else {
+                            r = q == 2u ? emit_pbvr(f, T, i, rs, R, S) : q;
+                        }
+                        exact_runs += q == 2u ? 1u : 0u;
+                    }
                     points += r & 1u;
                     writes += r >> 1;
                 } else {
@@ -659,27 +994,32 @@ __global__ void __launch_bounds__(kPT, GPSB_PARTICLE_MIN_BLOCKS) k_particles(Fra
         }
         __syncthreads();
     }
-    ull v = points, wv = writes;
+    ull v = points, wv = writes, xv = exact_runs, mv = mismatch;
     for (int o = 16; o; o >>= 1) {
         v += __shfl_xor_sync(0xffffffffu, v, o);
         wv += __shfl_xor_sync(0xffffffffu, wv, o);
+        xv += __shfl_xor_sync(0xffffffffu, xv, o);
+        mv += __shfl_xor_sync(0xffffffffu, mv, o);
     }
     if (lane == 0 && v && MC != 0) atomicAdd(&stats[ST_POINTS], v);
     if (lane == 0 && wv) atomicAdd(&stats[ST_WRITES], wv);
+    if (lane == 0 && xv) atomicAdd(&stats[ST_FAST_EXACT], xv);
+    if (lane == 0 && mv) atomicAdd(&stats[ST_FAST_MISMATCH], mv);
 }
 
-template <int MC, int IPT>
+template <int MC, int IPT, int FM>
 static void launch_particles_t(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,
                                const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
                                uint32_t* unit_counter, unsigned long long* stats, int grid, cudaStream_t st) {
     size_t smem = (kTabFloats + 2 * ((size_t)E + 1) + 2 * (kPT * IPT + 2)) * sizeof(uint32_t);
     if (MC == 0 && !fc.exact_radius) smem += kLutN * sizeof(float);
+    if (MC == 1 && FM == 1) smem += (size_t)(kPT / 32) * kRing * sizeof(uint2);
     static size_t attr = 0;
     if (smem > 48 * 1024 && smem > attr) {
-        cudaFuncSetAttribute(k_particles<MC, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_particles<MC, IPT, FM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = smem;
     }
-    k_particles<MC, IPT><<<grid, kPT, smem, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
+    k_particles<MC, IPT, FM><<<grid, kPT, smem, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
 }
 
 template <int IPT>
@@ -687,11 +1027,15 @@ static void launch_particles_m(const FrameConst& fc, const float4* rec, const fl
                                const EnsTotal* etot, uint32_t first_seed, uint32_t E, unsigned long long* sub,
                                uint32_t* unit_counter, unsigned long long* stats, int grid, cudaStream_t st) {
     if (fc.method == 0u)
-        launch_particles_t<0, IPT>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+        launch_particles_t<0, IPT, 0>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
     else if (fc.method == 4u)
-        launch_particles_t<2, IPT>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+        launch_particles_t<2, IPT, 0>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+    else if (fc.fast_mode == 1u)
+        launch_particles_t<1, IPT, 1>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+    else if (fc.fast_mode == 2u)
+        launch_particles_t<1, IPT, 2>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
     else
-        launch_particles_t<1, IPT>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
+        launch_particles_t<1, IPT, 0>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats, grid, st);
 }
 
 void launch_particles(const FrameConst& fc, const float4* rec, const float* lut, const uint2* clist,

@@ -102,6 +102,9 @@ struct gpsb_renderer {
     // footprint-subpixel Monte-Carlo mode (GPS)
     uint32_t fp_fixed = 1, fp_max = 4, fp_comp = 0;
     float fp_kappa = 0.0f;
+    // PBVR fast decisions: 0 off, 1 on (default), 2 validate
+    uint32_t fast_mode = 1;
+    DevBuf dbg;
     // captured trajectory pipeline (gpsb_render_trajectory_graph) and the key of its work
     cudaGraphExec_t traj_exec = nullptr;
     std::vector<uint8_t> traj_key;
@@ -210,6 +213,7 @@ static FrameConst make_frame(const gpsb_renderer* r, const gpsb_camera& cam, con
     f.fp_max = r->fp_max;
     f.fp_comp = r->fp_comp;
     f.fp_kappa = r->fp_kappa;
+    f.fast_mode = r->fast_mode;
     return f;
 }
 
@@ -467,6 +471,7 @@ void gpsb_destroy(gpsb_renderer* r) {
     sorted_release(r->sorted);
     r->prim_lookback.release();
     r->prim_counter.release();
+    r->dbg.release();
     radix_release(r->prim_sort);
     for (auto& pe : r->pending) {
         cudaEventDestroy(pe.a);
@@ -489,6 +494,35 @@ gpsb_status gpsb_set_footprint(gpsb_renderer* r, uint32_t footprint_subpixels, f
     r->fp_max = std::max(footprint_max, 1u);
     r->fp_comp = compensate_blur ? 1u : 0u;
     r->fp_kappa = adaptive_kappa;
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_set_fast_decisions(gpsb_renderer* r, uint32_t mode) {
+    if (!r) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null renderer");
+    if (mode > 2) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "fast decision mode must be 0 (off), 1 (on) or 2 (validate)");
+    r->fast_mode = mode;
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_debug_fast_counts(gpsb_renderer* r, uint64_t* counts) {
+    if (!r || !counts) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null renderer or output");
+    cudaSetDevice(r->device);
+    unsigned long long w[ST_WORDS];
+    CK(r, cudaMemcpyAsync(w, r->stats.p, sizeof w, cudaMemcpyDeviceToHost, r->stream), "read stats");
+    CK(r, cudaStreamSynchronize(r->stream), "synchronise");
+    counts[0] = w[ST_FAST_EXACT];
+    counts[1] = w[ST_FAST_MISMATCH];
+    return check_error_word(r);
+}
+
+gpsb_status gpsb_debug_fast_bounds(gpsb_renderer* r, float* ratios) {
+    if (!r || !ratios) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null renderer or output");
+    cudaSetDevice(r->device);
+    CK(r, r->dbg.ensure(64), "debug scratch");
+    launch_fast_bounds((uint32_t*)r->dbg.p, r->stream);
+    CK(r, cudaGetLastError(), "fast bounds launch");
+    CK(r, cudaMemcpyAsync(ratios, r->dbg.p, 6 * sizeof(float), cudaMemcpyDeviceToHost, r->stream), "read ratios");
+    CK(r, cudaStreamSynchronize(r->stream), "synchronise");
     return GPSB_OK;
 }
 
@@ -682,9 +716,12 @@ gpsb_status gpsb_render_trajectory_graph(gpsb_renderer* r, const gpsb_camera* ca
     auto put = [&](const void* d, size_t n) { key.insert(key.end(), (const uint8_t*)d, (const uint8_t*)d + n); };
     put(cams, sizeof(gpsb_camera) * n_cams);
     put(p, sizeof *p);
+    uint32_t kappa_bits;
+    memcpy(&kappa_bits, &r->fp_kappa, 4);
     uint64_t misc[] = {first_seed, E, (uint64_t)(uintptr_t)accum_out_dev, r->scene_gen, r->W, r->H, r->side,
                        r->particle_items, r->particle_blocks_per_sm, r->ensemble_batch, (uint64_t)r->sorted.digit_bits,
-                       (uint64_t)(uintptr_t)r->stream};
+                       (uint64_t)(uintptr_t)r->stream, r->fp_fixed, r->fp_max, r->fp_comp,
+                       (uint64_t)kappa_bits, r->fast_mode};
     put(misc, sizeof misc);
     // the device buffers baked into the graph: a reallocation (bigger batch, new scene or frame
     // size) must re-capture, never replay stale pointers

@@ -442,6 +442,22 @@ class GpsRenderer:
         self._ck(self._L.gpsb_set_footprint(self._r, footprint_subpixels, adaptive_kappa, footprint_max,
                                             int(bool(compensate_blur))))
 
+    def set_fast_decisions(self, mode: int = 1):
+        """PBVR fast decisions: 0 off, 1 on (outputs bit-identical), 2 validate every particle."""
+        self._ck(self._L.gpsb_set_fast_decisions(self._r, int(mode)))
+
+    def debug_fast_counts(self):
+        """(particles left to the exact path, fast answers that disagreed) of the last frame."""
+        out = np.zeros(2, np.uint64)
+        self._ck(self._L.gpsb_debug_fast_counts(self._r, out.ctypes.data_as(C.c_void_p)))
+        return int(out[0]), int(out[1])
+
+    def debug_fast_bounds(self) -> np.ndarray:
+        """Largest error / bound of each approximation the fast decisions use, over all its inputs."""
+        out = np.zeros(6, np.float32)
+        self._ck(self._L.gpsb_debug_fast_bounds(self._r, out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def set_feature_accum(self, feat):
         """Denoiser feature sums into `feat` (a zeroed CUDA tensor of W*H*8 float32), or None to stop."""
         self._ck(self._L.gpsb_set_feature_accum(self._r, C.c_void_p(feat.data_ptr()) if feat is not None else None))

@@ -178,6 +178,20 @@ gpsb_status gpsb_set_stream(gpsb_renderer* r, void* cuda_stream);
  * blur. footprint_subpixels <= 1 with adaptive_kappa = 0 is the normal GPS renderer. */
 gpsb_status gpsb_set_footprint(gpsb_renderer* r, uint32_t footprint_subpixels, float adaptive_kappa,
                               uint32_t footprint_max, uint32_t compensate_blur);
+/* PBVR fast decisions (no counterpart in the reference, whose shader runs every particle through
+ * the full path): 0 off; 1 on, where particles that bounded approximate maths proves are not
+ * points or are points off screen skip the exact path, which leaves every output bit-identical;
+ * 2 validate, where every particle runs the exact path and the fast answer is checked against it
+ * (gpsb_debug_fast_counts). Default 1. */
+gpsb_status gpsb_set_fast_decisions(gpsb_renderer* r, uint32_t mode);
+/* Of the last frame: counts[0] = particles the fast decisions left to the exact path, counts[1] =
+ * fast answers that disagreed with the exact path (mode 2; always 0 when the bounds hold). */
+gpsb_status gpsb_debug_fast_counts(gpsb_renderer* r, uint64_t* counts);
+/* Exhaustive check of the fast decisions' approximation constants over every input they can get:
+ * ratios[0..5] = largest |approximation - exact| / bound of log (uniforms), log ([1e-6, 1)),
+ * sin/cos, the Box-Muller radius, the radius' maximum, exp ([-128, 0]); each <= 1 when the bounds
+ * hold. */
+gpsb_status gpsb_debug_fast_bounds(gpsb_renderer* r, float* ratios);
 /* Denoiser features (no counterpart in the reference, which has no denoiser): with feat_dev set
  * (device memory of the caller, width*height*8 floats, zeroed by the caller), every rendered
  * ensemble also adds, per pixel, (r^2, g^2, b^2, alpha, depth) of its resolved colour, covered
