@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -64,6 +65,7 @@ struct gpsb_renderer {
     int sm_count = 148;
     // scene
     DevBuf splats, sh, lut;
+    DevBuf spare[5];  // staging set of splats, sh, rec, cdesc, colour for the next scene
     // per camera
     DevBuf rec, cdesc, colour;
     // per frame
@@ -468,6 +470,7 @@ void gpsb_destroy(gpsb_renderer* r) {
     DevBuf* bufs[] = {&r->splats, &r->sh, &r->lut, &r->rec, &r->cdesc, &r->colour, &r->accum, &r->stats, &r->err,
                       &r->sub, &r->clist, &r->lookback, &r->etot, &r->counters, &r->rgba8};
     for (DevBuf* b : bufs) b->release();
+    for (DevBuf& b : r->spare) b.release();
     sorted_release(r->sorted);
     r->prim_lookback.release();
     r->prim_counter.release();
@@ -564,24 +567,21 @@ static gpsb_status set_scene(gpsb_renderer* r, const void* g, size_t n, const fl
         }
         deg = d;
     }
-    // Stage into fresh buffers so a failure keeps the old scene (gps.rs:682).
-    DevBuf ns, nsh, nrec, ncd, ncol;
+    // Stage into the spare set of scene buffers so a failure keeps the old scene (gps.rs:682); the
+    // sets swap afterwards, so reloading a scene of the same size allocates nothing.
+    DevBuf &ns = r->spare[0], &nsh = r->spare[1], &nrec = r->spare[2], &ncd = r->spare[3], &ncol = r->spare[4];
     cudaError_t e;
     if ((e = ns.ensure(std::max<size_t>(n, 1) * 64)) != cudaSuccess ||
         (e = nsh.ensure(deg ? (size_t)n * 3 * stride * 4 : 64)) != cudaSuccess ||
         (e = nrec.ensure(std::max<size_t>(n, 1) * kRecF4 * 16)) != cudaSuccess ||
         (e = ncd.ensure(std::max<size_t>(n, 1) * 8)) != cudaSuccess ||
         (e = ncol.ensure(std::max<size_t>(n, 1) * 16)) != cudaSuccess) {
-        ns.release(); nsh.release(); nrec.release(); ncd.release(); ncol.release();
         return cuda_fail(r, e, "scene buffers");
     }
     if (n) e = cudaMemcpyAsync(ns.p, g, n * 64, kind, r->stream);
     if (e == cudaSuccess && deg) e = cudaMemcpyAsync(nsh.p, sh, (size_t)n * 3 * stride * 4, kind, r->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(r->stream);
-    if (e != cudaSuccess) {
-        ns.release(); nsh.release(); nrec.release(); ncd.release(); ncol.release();
-        return cuda_fail(r, e, "scene upload");
-    }
+    if (e != cudaSuccess) return cuda_fail(r, e, "scene upload");
     // centroid of the positions (gps.rs:731-735), from a host copy
     double c[3] = {0, 0, 0};
     if (n) {
@@ -589,24 +589,24 @@ static gpsb_status set_scene(gpsb_renderer* r, const void* g, size_t n, const fl
         const gpsb_gaussian* hg = (const gpsb_gaussian*)g;
         if (kind != cudaMemcpyHostToDevice) {
             host.resize(n);
-            if ((e = cudaMemcpy(host.data(), ns.p, n * 64, cudaMemcpyDeviceToHost)) != cudaSuccess) {
-                ns.release(); nsh.release(); nrec.release(); ncd.release(); ncol.release();
+            if ((e = cudaMemcpy(host.data(), ns.p, n * 64, cudaMemcpyDeviceToHost)) != cudaSuccess)
                 return cuda_fail(r, e, "centroid readback");
-            }
             hg = host.data();
         }
         for (size_t i = 0; i < n; ++i)
             for (int k = 0; k < 3; ++k) c[k] = c[k] + (double)hg[i].pos_opacity[k];
         for (int k = 0; k < 3; ++k) c[k] = c[k] / (double)n;
     }
-    r->splats.release(); r->sh.release(); r->rec.release(); r->cdesc.release(); r->colour.release();
-    r->splats = ns; r->sh = nsh; r->rec = nrec; r->cdesc = ncd; r->colour = ncol;
+    std::swap(r->splats, ns);
+    std::swap(r->sh, nsh);
+    std::swap(r->rec, nrec);
+    std::swap(r->cdesc, ncd);
+    std::swap(r->colour, ncol);
     r->n = (uint32_t)n;
     r->sh_max_degree = deg;
     r->sh_stride = stride;
     memcpy(r->centroid, c, sizeof c);
-    r->batch_cap = 0;
-    r->sub.release(); r->clist.release(); r->lookback.release(); r->etot.release();
+    r->batch_cap = 0;  // the per-ensemble buffers grow to the new scene on the next render
     r->have_sorted = false;
     r->scene_gen += 1;
     return gpsb_reset_accum(r);

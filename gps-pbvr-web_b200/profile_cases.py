@@ -5,6 +5,9 @@ runs a few launches of a case larger than the 126 MB L2 but a few GB at most on 
   sort           stable radix sort of 2^24 (24-bit key, value) pairs, 8-bit digits, 3 times (k_onesweep)
   denoise-train  two training steps of the denoiser on 2 x 256 x 256 crops (k_conv_fwd, k_conv_dw, ...)
   denoise-infer  two 1280 x 720 inferences of the denoiser
+  particles-near       PBVR Extinction C3+R, 560k-Gaussian cluster scene, 1280 x 720, near orbit view
+                       (distance 2.5), 2 ensembles in one launch of k_particles, fast decisions on
+  particles-near-exact the same with the fast decisions off (every particle on the exact path)
 
 python gps-pbvr-web_b200/profile_cases.py scan|sort|denoise-train|denoise-infer
 """
@@ -82,11 +85,30 @@ def denoise(pkg, train):
     return net.error_word()
 
 
+def particles_near(pkg, fast):
+    import torch
+    from gps_pbvr_web_b200 import scenes
+    splats, sh, deg = pkg.load_ply(scenes.cluster_scene(560_000, seed=0, degree=3))
+    w, h = 1280, 720
+    cam = pkg.OrbitCamera(target=(0.0, 0.0, 0.0), distance=2.5, yaw=0.6, pitch=0.25, up=(0.0, -1.0, 0.0),
+                          fov_y=0.9).to_camera(w, h)
+    p = pkg.RenderParams(spp_side=1, max_points_per_splat=16384, method=pkg.Method.Extinction)
+    p.pbvr.calibration = pkg.Calibration.PerSplatFootprint
+    p.pbvr.radial_correction = True
+    r = pkg.GpsRenderer(w, h, 1)
+    r.set_gaussians_sh(splats, sh, deg)
+    r.set_fast_decisions(1 if fast else 0)
+    r.render_ensembles(cam, p, 1, 2)
+    torch.cuda.synchronize()
+    return r.debug_error_word()
+
+
 def main(argv=None):
     case = (argv or sys.argv[1:] or ["scan"])[0]
     pkg = _pkg()
     fn = {"scan": scan, "sort": sort, "denoise-train": lambda p: denoise(p, True),
-          "denoise-infer": lambda p: denoise(p, False)}[case]
+          "denoise-infer": lambda p: denoise(p, False), "particles-near": lambda p: particles_near(p, True),
+          "particles-near-exact": lambda p: particles_near(p, False)}[case]
     err = fn(pkg)
     print(case, "error word", err)
     return 1 if err else 0
