@@ -128,37 +128,45 @@ __global__ void __launch_bounds__(kRsThreads, GPSB_SORT_MIN_BLOCKS) k_onesweep(c
     }
     uint32_t key[kRsIpt], rank[kRsIpt];
     const uint32_t lt = lanemask_lt();
+    uint32_t* wc = s_wcnt[warp];
     // rank every key within its warp's sub-tile in input order (stable): the lanes holding one digit
-    // find each other (peers: one ballot per digit bit, or match.any), the lowest of them adds the
-    // group's size to the warp's running count of that digit with a shared-memory atomic and
-    // passes the old count to its peers
-#pragma unroll
-    for (int q = 0; q < kRsIpt; ++q) {
-        uint32_t idx = base + q * 32 + lane;
-        bool valid = idx < n;
-        key[q] = valid ? __ldg(&kin[idx]) : 0u;
-        uint32_t d = valid ? ((key[q] >> shift) & (BINS - 1)) : (uint32_t)BINS;
-        // peer groups alternate between the ballot form (ALU pipe) and match.any (ADU pipe) so
-        // that neither pipe alone bounds the pass
+    // find each other (peers: one ballot per digit bit, or match.any), every lane reads its digit's
+    // running count of the warp, and the lowest lane of each group adds the group's size (the
+    // groups hold distinct digits, so the warp's counter row needs no atomics)
+    auto rank_key = [&](int q, uint32_t d, uint32_t live) {
         uint32_t peers;
         if (GPSB_SORT_BALLOT_PEERS == 1 || (GPSB_SORT_BALLOT_PEERS == 2 && (q & 1))) {
-            peers = __ballot_sync(0xffffffffu, valid);
+            peers = live;
 #pragma unroll
             for (int b = 0; b < BITS; ++b) {
-                const uint32_t bit = (d >> b) & 1u;
-                const uint32_t m = __ballot_sync(0xffffffffu, bit);
-                peers &= ~(m ^ (0u - bit));
+                const bool bs = (d >> b) & 1u;
+                const uint32_t m = __ballot_sync(0xffffffffu, bs);
+                peers &= bs ? m : ~m;
             }
-            if (!valid) peers = 0u;
         } else {
-            peers = __match_any_sync(0xffffffffu, d);
+            peers = __match_any_sync(0xffffffffu, d) & live;
         }
-        int leader = peers ? __ffs(peers) - 1 : lane;
-        uint32_t old = 0u;
-        if (valid && leader == lane) old = atomicAdd(&s_wcnt[warp][d], (uint32_t)__popc(peers));
-        old = __shfl_sync(0xffffffffu, old, leader);
-        rank[q] = old + __popc(peers & lt);
-        __syncwarp();  // orders this key's count update before the next key's (other leader lanes)
+        const uint32_t below = __popc(peers & lt);
+        const uint32_t old = wc[d];
+        __syncwarp();
+        if (below == 0u && ((live >> lane) & 1u)) wc[d] = old + (uint32_t)__popc(peers);
+        __syncwarp();  // orders this key's count update before the next key's reads
+        rank[q] = old + below;
+    };
+    if (tile_n == (uint32_t)kRsTile) {
+#pragma unroll
+        for (int q = 0; q < kRsIpt; ++q) {
+            key[q] = __ldg(&kin[base + q * 32 + lane]);
+            rank_key(q, (key[q] >> shift) & (BINS - 1), 0xffffffffu);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < kRsIpt; ++q) {
+            const uint32_t idx = base + q * 32 + lane;
+            const bool valid = idx < n;
+            key[q] = valid ? __ldg(&kin[idx]) : 0u;
+            rank_key(q, valid ? ((key[q] >> shift) & (BINS - 1)) : 0u, __ballot_sync(0xffffffffu, valid));
+        }
     }
     __syncthreads();
     // per digit: exclusive prefix over warps and the tile count; publish the tile's aggregate early
@@ -232,15 +240,21 @@ __global__ void __launch_bounds__(kRsThreads, GPSB_SORT_MIN_BLOCKS) k_onesweep(c
     }
     __syncthreads();
     // coalesced write-out: consecutive threads write consecutive keys of each digit run
-    for (uint32_t i = tid; i < tile_n; i += kRsThreads) {
-        uint32_t k = s_key[i];
-        uint32_t pos = s_gbase[(k >> shift) & (BINS - 1)] + i;
+    auto write_one = [&](uint32_t i) {
+        const uint32_t k = s_key[i];
+        const uint32_t pos = s_gbase[(k >> shift) & (BINS - 1)] + i;
         if (pos < n) {
             kout[pos] = k;
             vout[pos] = s_vin[s_src[i]];
         } else {
             atomicOr(err, ERR_BAD_INDEX);
         }
+    };
+    if (tile_n == (uint32_t)kRsTile) {
+#pragma unroll
+        for (int q = 0; q < kRsIpt; ++q) write_one((uint32_t)(q * kRsThreads + tid));
+    } else {
+        for (uint32_t i = tid; i < tile_n; i += kRsThreads) write_one(i);
     }
 }
 
