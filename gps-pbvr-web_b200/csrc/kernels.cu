@@ -68,7 +68,7 @@ __device__ __forceinline__ float mlog(float x) { return mufu(x, 0) * kLn2; }
 __device__ __forceinline__ float mexp(float a) { return mufu(a * kLog2e, 1); }
 
 // Per-splat bounds of the fast path's camera coordinates (written by the geometry kernel into
-// r1.z = |fx| ecx, r1.w = |fy| ecy, r3.z = ecz, r3.w = |a| + 2|b| + |c|, r4.w = 2(|a| + |b|),
+// r1.z = |fx| ecx, r1.w = |fy| ecy, r3.z = kSafe ecz, r3.w = |a| + 2|b| + |c|, r4.w = 2(|a| + |b|),
 // r5.w = 2(|b| + |c|) for the conic (a, b, c) = (r2.w, r3.x, r3.y)). World w_j = centre_j +
 // sum_k L_jk u_k (2, 4, 6 operations), p = w - camera (one more), c_i = dot3(rot_i, p) (5 more).
 __device__ __forceinline__ void fast_bounds_of(const FrameConst& f, float3 g0, float k00, float k10, float k11,
@@ -86,7 +86,7 @@ __device__ __forceinline__ void fast_bounds_of(const FrameConst& f, float3 g0, f
     const float ecx = row(f.rot0), ecy = row(f.rot1), ecz = row(f.rot2);
     r1.z = fabsf(f.fx) * ecx * F_(1.02);
     r1.w = fabsf(f.fy) * ecy * F_(1.02);
-    r3.z = ecz;
+    r3.z = ecz * kSafe;
     r3.w = (fabsf(a) + F_(2.0) * fabsf(b) + fabsf(c)) * F_(1.02);
     r4.w = F_(2.0) * (fabsf(a) + fabsf(b)) * F_(1.02);
     r5.w = F_(2.0) * (fabsf(b) + fabsf(c)) * F_(1.02);
@@ -578,10 +578,12 @@ __device__ __forceinline__ uint32_t emit_pbvr(const FrameConst& f, const FTabs& 
 // Returns false when x = -2 log u1 is below kXMin, where the kEN bound does not hold.
 __device__ __forceinline__ bool fast_pair(uint32_t& st, float& c, float& s) {
     const float u1 = fmax_(gx::next_u(&st), gxc::kUMin);
-    const float u2 = gx::next_u(&st);
-    const float x = -F_(2.0) * mlog(u1);
+    st = gx::pcg(st);  // u2 = (st >> 8) 2^-24, folded into t below
+    // x = -2 mlog(u1) and t = RN(2 pi u2), each with one rounding: scaling by a power of two
+    // commutes with rounding, so both equal the two-step values bit for bit
+    const float x = mufu(u1, 0) * (-F_(2.0) * kLn2);
     const float r = x * mufu(x, 2);
-    const float t = gxc::kTwoPi * u2;
+    const float t = (float)(st >> 8u) * (gxc::kTwoPi * (F_(1.0) / F_(16777216.0)));
     c = r * mufu(t, 5);
     s = r * mufu(t, 4);
     return x >= kXMin;
@@ -602,7 +604,7 @@ __device__ __forceinline__ uint32_t pbvr_fast(const FrameConst& f, uint32_t st, 
     const float py = __fmaf_rn(r4.z, uy, __fmaf_rn(r4.y, ux, r2.y)) - f.pos[1];
     const float pz = __fmaf_rn(r5.z, uz, __fmaf_rn(r5.y, uy, __fmaf_rn(r5.x, ux, r2.z))) - f.pos[2];
     const float cz = __fmaf_rn(f.rot2[2], pz, __fmaf_rn(f.rot2[1], py, f.rot2[0] * px));
-    const float ecz = r3.z * kSafe;
+    const float ecz = r3.z;  // already widened by kSafe
     const bool behind = cz + ecz <= f.near_z;  // surely not a point
     const float czl = cz - ecz;
     bool sure = czl > f.near_z && czl > F_(3.0) * ecz && cz < 1e30f && czl > 1e-6f;  // surely in front
@@ -612,7 +614,7 @@ __device__ __forceinline__ uint32_t pbvr_fast(const FrameConst& f, uint32_t st, 
     // paths' roundings (1e-6 |t|), 1 / (cz - ecz) <= (1 + 2 ecz / cz) / cz for ecz <= cz / 4;
     // then + f.cx with one more rounding in each path
     const float icz = mufu(cz, 3);
-    const float icl = icz * __fmaf_rn(F_(2.0) * ecz, icz, F_(1.0)) * kSafe;
+    const float icl = icz * __fmaf_rn((F_(2.0) * kSafe) * ecz, icz, kSafe);
     const float kt = __fmaf_rn(ecz, icl, 1e-6f + F_(2.0) * kU);
     const float tx = (f.fx * cx) * icz, ty = (f.fy * cy) * icz;
     float pix_x = tx + f.cx, pix_y = ty + f.cy;
@@ -644,14 +646,14 @@ __device__ __forceinline__ uint32_t pbvr_fast(const FrameConst& f, uint32_t st, 
         const float r2v = __fmaf_rn(r2.w, dx2, __fmaf_rn(F_(2.0) * r3.x, dvx * dvy, r3.y * dy2));
         const float m2 = __fmaf_rn(r4.w, dx2, r5.w * dy2);
         const float er2 = __fmaf_rn(__fmaf_rn(r4.w, fabsf(dvx), r5.w * fabsf(dvy)), e, __fmaf_rn(r3.w * e, e, F_(10.0) * kU * m2));
-        const float arg = -F_(0.5) * fmaxf(r2v, F_(0.0));
-        const float earg = F_(0.5) * er2 * kSafe;
+        const float a2 = fmaxf(r2v, F_(0.0));  // arg = -a2 / 2
+        const float earg = er2 * (F_(0.5) * kSafe);
         // y = min(o, 1 - 1e-6) exp(arg): propagated error (e^earg - 1 <= earg (1 + earg)), the
         // approximation against exp, exp's own 2 ulp at both arguments, the product's roundings;
         // with earg < 1/8 every relative term grows by at most (1 + 2 earg) <= 1.25
         const float oo = fmin_(r0.w, gxc::kOneMinus1e6);
-        const float y = oo * mexp(arg);
-        const float rel = __fmaf_rn(earg, F_(1.0) + earg, __fmaf_rn(kExpB, fabsf(arg), kExpA + F_(5.4e-7) + F_(2.0) * kU));
+        const float y = oo * mufu(a2 * (-F_(0.5) * kLog2e), 1);  // = mexp(arg) bit for bit
+        const float rel = __fmaf_rn(earg, F_(1.0) + earg, __fmaf_rn(F_(0.5) * kExpB, a2, kExpA + F_(5.4e-7) + F_(2.0) * kU));
         const float ey = __fmaf_rn(y, rel * (F_(1.25) * kSafe), F_(2.02) * kExpTiny);
         // eol's short form (both paths take it when y + ey < 1e-4) ...
         const bool small = y + ey < F_(1e-4);
