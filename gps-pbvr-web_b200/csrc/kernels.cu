@@ -803,7 +803,7 @@ __global__ void __launch_bounds__(kPT, FM == 1 ? GPSB_FAST_MIN_BLOCKS : GPSB_PAR
     uint32_t* s_off = s_dyn + kTabFloats + 2 * (E + 1);
     uint32_t* s_id = s_off + (kPTile + 2);
     float* s_lut = reinterpret_cast<float*>(s_id + (kPTile + 2));
-    __shared__ uint32_t s_unit, s_j0, s_w;
+    __shared__ uint32_t s_unit, s_j0, s_w, s_claim;
     const int tid = threadIdx.x, lane = tid & 31;
     const bool use_lut = MC == 0 && !f.exact_radius;
     if (use_lut)
@@ -821,11 +821,37 @@ __global__ void __launch_bounds__(kPT, FM == 1 ? GPSB_FAST_MIN_BLOCKS : GPSB_PAR
     const uint64_t total_units = s_ubase[E];
     const uint64_t PS = (uint64_t)f.W * f.H * f.S;
     uint32_t points = 0, writes = 0, exact_runs = 0, mismatch = 0;
+    // next tile: its unit number and list window, found by one warp (lane 0 writes s_unit, s_j0, s_w)
+    auto find_unit = [&]() {
+        uint32_t un = 0u;
+        if (lane == 0) un = atomicAdd(unit_counter, 1u);
+        un = __shfl_sync(0xffffffffu, un, 0);
+        uint32_t j0 = 0u, j1 = 0u;
+        if ((uint64_t)un < total_units) {
+            uint32_t lo = 0, hi = E;
+            while (hi - lo > 1u) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (s_ubase[mid] <= un) lo = mid; else hi = mid;
+            }
+            const EnsTotal et = etot[lo];
+            const uint64_t q0 = ((uint64_t)un - s_ubase[lo]) * kPTile;
+            const uint64_t q1 = q0 + kPTile < et.particles ? q0 + kPTile : et.particles;
+            const uint2* Lq = clist + (size_t)lo * f.N;
+            j0 = warp_last_le(Lq, 0u, et.nonzero, q0, lane);
+            j1 = warp_last_le(Lq, j0, et.nonzero, q1 - 1, lane);
+        }
+        if (lane == 0) {
+            s_unit = un;
+            s_j0 = j0;
+            s_w = j1 - j0 + 1u;
+        }
+    };
+    if (tid < 32) find_unit();
+    __syncthreads();
     for (;;) {
-        if (tid == 0) s_unit = atomicAdd(unit_counter, 1u);
-        __syncthreads();
         const uint64_t u = s_unit;
         if (u >= total_units) break;
+        const uint32_t j0 = s_j0, w = s_w;
         // ensemble of unit u: largest e with s_ubase[e] <= u
         uint32_t lo = 0, hi = E;
         while (hi - lo > 1u) {
@@ -837,13 +863,6 @@ __global__ void __launch_bounds__(kPT, FM == 1 ? GPSB_FAST_MIN_BLOCKS : GPSB_PAR
         const uint64_t p0 = (u - s_ubase[e]) * kPTile;
         const uint64_t p1 = p0 + kPTile < et.particles ? p0 + kPTile : et.particles;
         const uint2* L = clist + (size_t)e * f.N;
-        if (tid < 32) {
-            uint32_t j0 = warp_last_le(L, 0u, et.nonzero, p0, lane);
-            uint32_t j1 = warp_last_le(L, j0, et.nonzero, p1 - 1, lane);
-            if (lane == 0) { s_j0 = j0; s_w = j1 - j0 + 1u; }
-        }
-        __syncthreads();
-        const uint32_t j0 = s_j0, w = s_w;
         for (uint32_t q = tid; q <= w; q += kPT) {
             uint32_t j = j0 + q;
             if (q < w) {
@@ -854,7 +873,8 @@ __global__ void __launch_bounds__(kPT, FM == 1 ? GPSB_FAST_MIN_BLOCKS : GPSB_PAR
                 s_off[q] = j < et.nonzero ? __ldg(&L[j].y) : (uint32_t)et.particles;
             }
         }
-        __syncthreads();
+        if (tid == 0) s_claim = 0u;
+        __syncthreads();  // window staged, unit read by every thread, claim open
         const uint32_t seed = first_seed + e;
         ull* S = sub + (size_t)e * PS;
         uint64_t p = p0 + (uint64_t)tid * kPIPT;
@@ -994,6 +1014,10 @@ __global__ void __launch_bounds__(kPT, FM == 1 ? GPSB_FAST_MIN_BLOCKS : GPSB_PAR
                 }
             }
         }
+        // the first warp done with this tile finds the next one while the others still work
+        uint32_t claim = 0u;
+        if (lane == 0) claim = atomicExch(&s_claim, 1u);
+        if (__shfl_sync(0xffffffffu, claim, 0) == 0u) find_unit();
         __syncthreads();
     }
     ull v = points, wv = writes, xv = exact_runs, mv = mismatch;
