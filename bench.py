@@ -148,6 +148,22 @@ def committed_traffic(kernel):
     return None
 
 
+def issue_roofline(st, ms, world, clk):
+    """The particle kernel is bound by instruction issue, not HBM: generated particles per second
+    (live) x warp instructions per particle (ncu, committed) against the SMs' issue peak (148 SMs x
+    4 schedulers x one warp instruction per clock at the median SM clock sampled in the timed
+    region)."""
+    per = committed_traffic("k_particles_warp_inst_per_particle")
+    mhz = clk.get("sm_mhz") if clk else None
+    if not per or not mhz or not st.particles:
+        return None
+    achieved = st.particles / (ms / 1000.0) * per  # per GPU: st and ms are this rank's
+    peak = 148 * 4 * mhz * 1e6
+    return {"kernel": "k_particles", "unit": "warp instructions/s", "achieved": achieved, "peak": peak,
+            "frac": achieved / peak, "warp_inst_per_particle": per,
+            "note": "particles and time live; instructions per particle from ncu on the near view (estimate)"}
+
+
 # ------------------------------------------------------------------------------ CPU reference
 def cpu_reference(pkg, splats, fraction, threads, views_cams, first_seed=1):
     """O1 render_particles_3d (the C++ port of gps-core, with the GPU's per-splat cap) on the first
@@ -549,8 +565,11 @@ def run_b200(args, rank, world):
                 "gaussians_per_s": world * args.steps * len(cams) * ENS * len(splats) / (ms / 1000.0),
                 "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak,
                              "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic},
+                "issue_roofline": issue_roofline(st, ms, world, clk),
+                "generated_particles_per_s": world * st.particles / (ms / 1000.0),
                 "stages": stage_gbs, "clocks": clk, "gpu_launches": prof["total_launches"],
-                "stats_per_step": {"points": st.points / args.steps, "subpixel_writes": st.subpixel_writes / args.steps,
+                "stats_per_step": {"particles": st.particles / args.steps, "points": st.points / args.steps,
+                                   "subpixel_writes": st.subpixel_writes / args.steps,
                                    "list_entries": st.list_entries / args.steps,
                                    "truncated_splats": st.truncated_splats / args.steps,
                                    "skipped_ensembles": st.skipped_ensembles},

@@ -41,7 +41,7 @@ class StatsC(C.Structure):
                 ("visible_splats", C.c_uint64), ("orphan_subpixels", C.c_uint64), ("candidates", C.c_uint64),
                 ("undercovered_splats", C.c_uint64), ("skipped_ensembles", C.c_uint64), ("ensembles", C.c_uint64),
                 ("probe_demand", C.c_uint64), ("issue", C.c_uint32), ("_pad", C.c_uint32),
-                ("subpixel_writes", C.c_uint64), ("list_entries", C.c_uint64)]
+                ("subpixel_writes", C.c_uint64), ("list_entries", C.c_uint64), ("particles", C.c_uint64)]
 
 
 class ProfileC(C.Structure):

@@ -52,7 +52,7 @@ constexpr int kRecF4 = 6;
 enum : int {
     ST_POINTS = 0, ST_TRUNCATED = 1, ST_DROPPED = 2, ST_VISIBLE = 3, ST_ORPHAN = 4, ST_CANDIDATES = 5,
     ST_UNDERCOVERED = 6, ST_SKIPPED = 7, ST_ENSEMBLES = 8, ST_PROBE = 9, ST_WRITES = 10, ST_ENTRIES = 11,
-    ST_FAST_EXACT = 12, ST_FAST_MISMATCH = 13, ST_WORDS = 16
+    ST_FAST_EXACT = 12, ST_FAST_MISMATCH = 13, ST_PARTICLES = 14, ST_WORDS = 16
 };
 
 // Device error word bits (bounded waits that gave up).

@@ -447,6 +447,8 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(FrameConst f, const
         if (total > 0xFFFFFFFFull) {
             atomicOr(&etot[e].flags, 1u);
             atomicAdd(&stats[ST_SKIPPED], 1ull);
+        } else {
+            atomicAdd(&stats[ST_PARTICLES], (ull)total);
         }
     }
 }

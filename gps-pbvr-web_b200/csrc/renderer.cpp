@@ -361,6 +361,7 @@ static void to_stats(const unsigned long long* w, gpsb_stats* out, uint32_t issu
     out->_pad = 0;
     out->subpixel_writes = w[ST_WRITES];
     out->list_entries = w[ST_ENTRIES];
+    out->particles = w[ST_PARTICLES];
 }
 
 static void poll_stats(gpsb_renderer* r) {

@@ -114,12 +114,13 @@ class GpuStats:  # gps.rs:231-252
     issue: int = 0
     subpixel_writes: int = 0
     list_entries: int = 0
+    particles: int = 0
 
     @staticmethod
     def from_c(s: abi.StatsC) -> "GpuStats":
         return GpuStats(s.points, s.truncated_splats, s.dropped_points, s.visible_splats, s.orphan_subpixels,
                         s.candidates, s.undercovered_splats, s.skipped_ensembles, s.ensembles, s.probe_demand, s.issue,
-                        s.subpixel_writes, s.list_entries)
+                        s.subpixel_writes, s.list_entries, s.particles)
 
     def counters(self):
         """Every counter but the readback issue number (for equality checks between paths)."""

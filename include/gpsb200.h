@@ -113,6 +113,9 @@ typedef struct gpsb_stats {
      * per-ensemble compact particle lists; they size the algorithmic bytes of the kernels */
     uint64_t subpixel_writes;
     uint64_t list_entries;
+    /* no reference counterpart: particles generated (the per-ensemble totals of the scan, summed
+     * over the ensembles that were not skipped), on screen or not */
+    uint64_t particles;
 } gpsb_stats;
 
 /* Device-time profile of the renderer's kernels (no reference counterpart; the reference has

@@ -41,7 +41,7 @@ def test_params_default_matches_reference():
 def test_struct_layouts():
     assert C.sizeof(abi.Gaussian) == 64
     assert C.sizeof(abi.Camera) == 17 * 8
-    assert C.sizeof(abi.StatsC) == 12 * 8 + 8
+    assert C.sizeof(abi.StatsC) == 13 * 8 + 8
 
 
 def test_radius_lut_bit_identical_to_oracle():
