@@ -44,8 +44,24 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // ============================================================================ radix sort
 constexpr int kRsThreads = 256;
 constexpr int kRsWarps = kRsThreads / 32;
-constexpr int kRsIpt = 15;  // keys per thread: 3840 per tile, 37.5 KB of shared staging
-constexpr int kRsTile = kRsThreads * kRsIpt;
+// Keys per thread and resident blocks per SM of a onesweep pass, per digit width: 8-bit digits
+// take 25 keys per thread (6400 per tile, 62.5 KB of staging, 3 blocks per SM), whose longer
+// digit runs write out in fuller sectors (2^26 pairs: 15 keys 2.24 TB/s, 21 2.31, 23 2.41, 25
+// 2.47); 4- and 6-bit digits 15 (3840, 37.5 KB, 4 blocks per SM), where larger tiles gained nothing.
+#ifndef GPSB_SORT_IPT8
+#define GPSB_SORT_IPT8 25
+#endif
+#ifndef GPSB_SORT_IPT
+#define GPSB_SORT_IPT 15
+#endif
+template <int BITS>
+struct RsShape {
+    static constexpr int ipt = BITS >= 8 ? GPSB_SORT_IPT8 : GPSB_SORT_IPT;
+    static constexpr int tile = kRsThreads * ipt;
+    static constexpr size_t stage = (size_t)tile * 10;  // dynamic shared memory of one block
+    static constexpr int min_blocks = stage + 8 * 1024 > 56 * 1024 ? 3 : 4;
+    static_assert(tile % 4 == 0 && tile <= 65536, "tile staging layout");
+};
 constexpr int kMaxPasses = 8;
 #ifndef GPSB_SORT_LOOKAHEAD
 #define GPSB_SORT_LOOKAHEAD 8
@@ -53,9 +69,6 @@ constexpr int kMaxPasses = 8;
 constexpr int kRsLook = GPSB_SORT_LOOKAHEAD;  // predecessor tiles read per lookback round trip
 #ifndef GPSB_SORT_BALLOT_PEERS
 #define GPSB_SORT_BALLOT_PEERS 1  // 0 match.any, 1 ballots, 2 alternating per key
-#endif
-#ifndef GPSB_SORT_MIN_BLOCKS
-#define GPSB_SORT_MIN_BLOCKS 4
 #endif
 constexpr uint32_t kStAgg = 1u << 30, kStPre = 2u << 30, kStMask = (1u << 30) - 1u;
 
@@ -90,17 +103,21 @@ __global__ void k_radix_hist_scan(uint32_t* hist, int passes) {
 }
 
 template <int BITS>
-__global__ void __launch_bounds__(kRsThreads, GPSB_SORT_MIN_BLOCKS) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+__global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                          uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                          uint32_t n, int shift, const uint32_t* __restrict__ gstart,
                                                          uint32_t* lookback, uint32_t* tile_counter, uint32_t* err) {
     constexpr int BINS = 1 << BITS;
+    constexpr int kRsIpt = RsShape<BITS>::ipt, kRsTile = RsShape<BITS>::tile;
     __shared__ uint32_t s_wcnt[kRsWarps][BINS];  // per-warp digit counts, then exclusive prefix over warps
     __shared__ uint32_t s_dstart[BINS];          // tile-local exclusive prefix over digits
     __shared__ uint32_t s_gbase[BINS];           // global position of the digit's first key of this tile, minus s_dstart
-    __shared__ uint32_t s_key[kRsTile];                // keys in digit order
-    __shared__ uint16_t s_src[kRsTile];                // tile-local input index of each ordered key
-    __shared__ __align__(16) uint32_t s_vin[kRsTile];  // the tile's values in input order
+    // dynamic shared memory (RsShape::stage bytes): keys in digit order, the tile's values in input order
+    // (16-byte aligned for cp.async), the tile-local input index of each ordered key
+    extern __shared__ __align__(16) uint32_t s_stage[];
+    uint32_t* s_key = s_stage;
+    uint32_t* s_vin = s_stage + kRsTile;
+    uint16_t* s_src = reinterpret_cast<uint16_t*>(s_stage + 2 * kRsTile);
     __shared__ uint32_t s_wsum[kRsWarps];
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -265,13 +282,24 @@ void radix_release(RadixScratch& s) {
     s = RadixScratch();
 }
 
+// One onesweep pass; the staging lives in dynamic shared memory (above 48 KB for large tiles).
+template <int BITS>
+static void onesweep_launch(uint32_t tiles, const uint32_t* ik, const uint32_t* iv, uint32_t* ok, uint32_t* ov,
+                            uint32_t n, int shift, const uint32_t* gstart, uint32_t* lookback, uint32_t* counter,
+                            uint32_t* err, cudaStream_t st) {
+    // set on every launch: the attributes belong to the current device's context
+    cudaFuncSetAttribute(k_onesweep<BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RsShape<BITS>::stage);
+    cudaFuncSetAttribute(k_onesweep<BITS>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    k_onesweep<BITS><<<tiles, kRsThreads, RsShape<BITS>::stage, st>>>(ik, iv, ok, ov, n, shift, gstart, lookback, counter, err);
+}
+
 template <int BITS>
 static cudaError_t radix_impl(RadixScratch& s, uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, uint32_t n,
                               int key_bits, uint32_t* err, cudaStream_t st) {
     constexpr int BINS = 1 << BITS;
     int passes = std::max(1, (key_bits + BITS - 1) / BITS);
     if (passes > kMaxPasses) return cudaErrorInvalidValue;
-    uint32_t tiles = (n + kRsTile - 1) / kRsTile;
+    const uint32_t tiles = (n + RsShape<BITS>::tile - 1) / RsShape<BITS>::tile;
     size_t hb = (size_t)passes * BINS * 4, lbb = (size_t)passes * std::max(tiles, 1u) * BINS * 4;
     cudaError_t e;
     if (hb > s.hist_bytes) {
@@ -302,12 +330,9 @@ static cudaError_t radix_impl(RadixScratch& s, uint32_t* ka, uint32_t* va, uint3
         cudaMemcpyAsync(kb, ka, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
         cudaMemcpyAsync(vb, va, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
     }
-    // four resident blocks per SM need the largest shared-memory carveout (48 KB each)
-    cudaFuncSetAttribute(k_onesweep<BITS>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     for (int p = 0; p < passes; ++p) {
-        k_onesweep<BITS><<<tiles, kRsThreads, 0, st>>>(ik, iv, ok, ov, n, p * BITS, hist + p * BINS,
-                                                       (uint32_t*)s.lookback + (size_t)p * tiles * BINS,
-                                                       (uint32_t*)s.counters + p, err);
+        onesweep_launch<BITS>(tiles, ik, iv, ok, ov, n, p * BITS, hist + p * BINS,
+                              (uint32_t*)s.lookback + (size_t)p * tiles * BINS, (uint32_t*)s.counters + p, err, st);
         std::swap(ik, ok);
         std::swap(iv, ov);
     }
@@ -319,10 +344,10 @@ static cudaError_t radix_impl(RadixScratch& s, uint32_t* ka, uint32_t* va, uint3
 // budget through its own pool, or a real-time frame loop where a cudaMalloc would stall or is
 // forbidden) use gpsb_sort_pairs_noalloc. Its scratch (digit histograms, tile counters and the
 // lookback words) is this file-scope array, sized for kNoAllocMaxN pairs with up to 32-bit keys
-// (4 passes of 8-bit digits): about 2.2 MB that every GPU which loads the library keeps until the
+// (4 passes of 8-bit digits): about 1.35 MB that every GPU which loads the library keeps until the
 // process exits.
 constexpr uint32_t kNoAllocMaxN = 1u << 21;
-constexpr uint32_t kNoAllocTiles = (kNoAllocMaxN + kRsTile - 1) / kRsTile;
+constexpr uint32_t kNoAllocTiles = (kNoAllocMaxN + RsShape<8>::tile - 1) / RsShape<8>::tile;
 constexpr uint32_t kNoAllocPasses = 4;
 constexpr size_t kNoAllocHistWords = kNoAllocPasses * 256;
 constexpr size_t kNoAllocCounterWords = 16;  // per-pass tile counters, then the default error word
@@ -806,7 +831,7 @@ extern "C" gpsb_status gpsb_sort_pairs_noalloc(uint32_t* keys_in, uint32_t* vals
         return GPSB_ERR_CUDA;
     }
     const int passes = (int)((key_bits + 7) / 8);
-    const uint32_t tiles = (n + kRsTile - 1) / kRsTile;
+    const uint32_t tiles = (n + RsShape<8>::tile - 1) / RsShape<8>::tile;
     uint32_t* hist = base;
     uint32_t* counters = base + kNoAllocHistWords;
     uint32_t* err = err_dev ? err_dev : counters + kNoAllocPasses;
@@ -825,8 +850,8 @@ extern "C" gpsb_status gpsb_sort_pairs_noalloc(uint32_t* keys_in, uint32_t* vals
         k_radix_hist<8><<<std::min<uint32_t>((n + 4095) / 4096, 1184u), 256, 0, st>>>(ik, n, passes, hist);
         k_radix_hist_scan<8><<<1, 32, 0, st>>>(hist, passes);
         for (int p = 0; p < passes; ++p) {
-            k_onesweep<8><<<tiles, kRsThreads, 0, st>>>(ik, iv, ok, ov, n, p * 8, hist + p * 256,
-                                                        lookback + (size_t)p * tiles * 256, counters + p, err);
+            onesweep_launch<8>(tiles, ik, iv, ok, ov, n, p * 8, hist + p * 256, lookback + (size_t)p * tiles * 256,
+                               counters + p, err, st);
             std::swap(ik, ok);
             std::swap(iv, ov);
         }

@@ -336,7 +336,7 @@ gpsb_status gpsb_p0_sample(gpsb_renderer* r, uint32_t seed, uint32_t pixel_base,
  * stall or is not allowed. It allocates nothing: all four pointers are device memory of the
  * caller; the sorted pairs are written to keys_out/vals_out and keys_in/vals_in are overwritten
  * (they are the ping-pong buffer). Its scratch is a fixed array inside this library (about
- * 2.2 MB, held by every GPU that loads the library until the process exits), which limits n to
+ * 1.35 MB, held by every GPU that loads the library until the process exits), which limits n to
  * 2,097,152 pairs; larger n returns GPSB_ERR_LIMIT. The first call on a device looks the array's
  * device address up (cudaGetSymbolAddress, with that device current); make that first call
  * before any stream capture. Work is enqueued on cuda_stream (NULL = the legacy default stream)
