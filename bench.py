@@ -1,8 +1,8 @@
 """Benchmark of the stochastic particle-rendering path on B200.
 
-Workload: 560,000 synthetic Gaussians (64 anisotropic clusters + 10%
-background, SH degree 3), PBVR Extinction C3+R, spp 1, per-splat cap 16,384, 1280x720, 64
-ensembles at each of three orbit distances (near 2.5, mid 7, far 20). One step renders the 64
+Workload (the reference's 560k-Gaussian benchmark configuration, synthesised): 560,000 synthetic
+Gaussians (64 anisotropic clusters + 10% background, SH degree 3), PBVR Extinction C3+R, spp 1,
+per-splat cap 16,384, 1280x720, 64 ensembles at each of three orbit distances (near 2.5, mid 7, far 20). One step renders the 64
 ensembles of all three views (192 ensembles); the metric is whole-job ensembles per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
@@ -290,7 +290,7 @@ def micro_scan_sort(pkg, r, stream, peak):
 
 
 def denoise_measure(pkg, r, stream, cams, p, per_view_ms, ref_ens=256):
-    """BASELINE's "ms to PSNR vs the 256-ensemble reference: denoised batch vs plain", per view:
+    """The "ms to PSNR vs the 256-ensemble reference: denoised batch vs plain" comparison, per view:
     the 4-ensemble frame through the trained denoiser (committed weights) against the plain
     accumulation. PSNR (peak 1, linear RGB clamped to [0, 1]) against a 256-ensemble reference with
     disjoint seeds; the plain path's PSNR is measured at 4..128 ensembles and the ensembles it

@@ -1,4 +1,4 @@
-"""Multi-GPU plumbing of the renderer: ensembles are independent, so N ranks (one
+"""Multi-GPU plumbing of the renderer: ensembles are independent of each other, so N ranks (one
 process per GPU) split the ensembles of every camera and need no collective on the data path.
 The only exchange is optional: summing the ranks' accumulations into one history, a single
 all-reduce of W*H*4 floats (NCCL over NVLink on GPUs, gloo in the CPU tests).

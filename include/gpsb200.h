@@ -399,7 +399,7 @@ gpsb_status gpsb_session_frame(gpsb_session* s, double now_ms, int* presented);
 gpsb_status gpsb_session_read_state(const gpsb_session* s, gpsb_session_state* out);
 
 /* ------------------------------------------------------------------- denoiser kernels
- * The learned denoiser of few-ensemble frames (BASELINE's "denoised batch vs plain"). The
+ * The learned denoiser of few-ensemble frames (the "denoised batch vs plain" comparison). The
  * reference has no denoiser, so none of these has a counterpart in it. All pointers are device
  * memory; activations are NHWC (pixel-major, channels innermost) bf16 with channel counts padded
  * to multiples of 8; weights are (cout, kp) bf16 rows, k = (ky*3 + kx)*cin + ci, kp a multiple of
