@@ -2,8 +2,9 @@
 
 Workload (the reference's 560k-Gaussian benchmark configuration, synthesised): 560,000 synthetic
 Gaussians (64 anisotropic clusters + 10% background, SH degree 3), PBVR Extinction C3+R, spp 1,
-per-splat cap 16,384, 1280x720, 64 ensembles at each of three orbit distances (near 2.5, mid 7, far 20). One step renders the 64
-ensembles of all three views (192 ensembles); the metric is whole-job ensembles per second.
+per-splat cap 16,384, 1280x720, 64 ensembles at each of three orbit distances (near 2.5, mid 7,
+far 20). One step renders the 64 ensembles of all three views (192 ensembles); the metric is
+whole-job ensembles per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
