@@ -171,9 +171,10 @@ __global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesw
         rank[q] = old + below;
     };
     if (tile_n == (uint32_t)kRsTile) {
+        const uint32_t* kp = kin + base + lane;  // the keys of this lane, 32 apart
 #pragma unroll
         for (int q = 0; q < kRsIpt; ++q) {
-            key[q] = __ldg(&kin[base + q * 32 + lane]);
+            key[q] = __ldg(kp + q * 32);
             rank_key(q, (key[q] >> shift) & (BINS - 1), 0xffffffffu);
         }
     } else {
@@ -257,14 +258,16 @@ __global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesw
     }
     __syncthreads();
     // coalesced write-out: consecutive threads write consecutive keys of each digit run
+    // (a position past n would mean corrupt histograms: it is skipped and reported once per thread)
+    bool bad = false;
     auto write_one = [&](uint32_t i) {
         const uint32_t k = s_key[i];
         const uint32_t pos = s_gbase[(k >> shift) & (BINS - 1)] + i;
-        if (pos < n) {
+        const bool ok = pos < n;
+        bad |= !ok;
+        if (ok) {
             kout[pos] = k;
             vout[pos] = s_vin[s_src[i]];
-        } else {
-            atomicOr(err, ERR_BAD_INDEX);
         }
     };
     if (tile_n == (uint32_t)kRsTile) {
@@ -273,6 +276,7 @@ __global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesw
     } else {
         for (uint32_t i = tid; i < tile_n; i += kRsThreads) write_one(i);
     }
+    if (bad) atomicOr(err, ERR_BAD_INDEX);
 }
 
 void radix_release(RadixScratch& s) {
