@@ -919,26 +919,26 @@ __global__ void __launch_bounds__(kPT, FM == 1 ? GPSB_FAST_MIN_BLOCKS : GPSB_PAR
                 ck = pp - s_off[jj];
                 nxt = s_off[jj + 1];
             }
-            for (int it = 0; it < kPIPT; ++it) {
-                uint32_t need = 0u, i = 0u, k = 0u;
-                if (pp < pend) {
-                    if (pp >= nxt) {
-                        while (pp >= s_off[jj + 1]) ++jj;
-                        ci = s_id[jj];
-                        ck = pp - s_off[jj];
-                        nxt = s_off[jj + 1];
-                    }
-                    i = ci;
-                    k = ck++;
-                    ++pp;
-                    if (fast) {
-                        if (i != cur) load_rec(i);
-                        const uint32_t q = pbvr_fast(f, gx::particle_seed(i, k + 1u, seed), R);
-                        if (q == 2u) need = 1u; else points += q;
-                    } else {
-                        run_exact(i, k);
-                    }
+            // fast steps: every lane evaluates a particle (a lane past its range evaluates one it
+            // does not own and ignores the answer; pbvr_fast only reads registers), so the step
+            // body has no divergent branch but the list boundary; a warp whose splat changed in
+            // any lane reloads every lane's record
+            int it = 0;
+            for (; it < kPIPT && fast; ++it) {
+                const bool act = pp < pend;
+                if (act && pp >= nxt) {
+                    while (pp >= s_off[jj + 1]) ++jj;
+                    ci = s_id[jj];
+                    ck = pp - s_off[jj];
+                    nxt = s_off[jj + 1];
                 }
+                const uint32_t i = ci, k = ck;
+                ck += act ? 1u : 0u;
+                pp += act ? 1u : 0u;
+                if (__any_sync(0xffffffffu, i != cur)) load_rec(i);
+                const uint32_t q = pbvr_fast(f, gx::particle_seed(i, k + 1u, seed), R);
+                const uint32_t need = (act && q == 2u) ? 1u : 0u;
+                points += (act && q != 2u) ? q : 0u;
                 const uint32_t bal = __ballot_sync(0xffffffffu, need);
                 if (bal == 0u) continue;
                 const uint32_t n = (uint32_t)__popc(bal);
@@ -948,11 +948,24 @@ __global__ void __launch_bounds__(kPT, FM == 1 ? GPSB_FAST_MIN_BLOCKS : GPSB_PAR
                 if (n > kFastGiveUp) fast = false;
                 if (count >= 32u) {
                     __syncwarp();
-                    const uint2 q = ring[(head + (uint32_t)lane) & (kRing - 1u)];
+                    const uint2 e = ring[(head + (uint32_t)lane) & (kRing - 1u)];
                     __syncwarp();
                     head += 32u;
                     count -= 32u;
-                    run_exact(q.x, q.y);
+                    run_exact(e.x, e.y);
+                }
+            }
+            // the rest of the tile on the exact path (after the warp gave the fast test up)
+            for (; it < kPIPT; ++it) {
+                if (pp < pend) {
+                    if (pp >= nxt) {
+                        while (pp >= s_off[jj + 1]) ++jj;
+                        ci = s_id[jj];
+                        ck = pp - s_off[jj];
+                        nxt = s_off[jj + 1];
+                    }
+                    run_exact(ci, ck++);
+                    ++pp;
                 }
             }
             __syncwarp();
