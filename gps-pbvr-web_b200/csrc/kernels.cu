@@ -657,25 +657,21 @@ __device__ __forceinline__ uint32_t pbvr_fast(const FrameConst& f, uint32_t st, 
         const float y = oo * mufu(a2 * (-F_(0.5) * kLog2e), 1);  // = mexp(arg) bit for bit
         const float rel = __fmaf_rn(earg, F_(1.0) + earg, __fmaf_rn(F_(0.5) * kExpB, a2, kExpA + F_(5.4e-7) + F_(2.0) * kU));
         const float ey = __fmaf_rn(y, rel * (F_(1.25) * kSafe), F_(2.02) * kExpTiny);
-        // eol's short form (both paths take it when y + ey < 1e-4) ...
-        const bool small = y + ey < F_(1e-4);
-        const float eo_s = F_(1.0) + F_(0.5) * y;
-        const float eeo_s = __fmaf_rn(F_(0.5), ey, F_(2.0) * kU * eo_s);
-        // ... and its log form, eol(y) = -log(1 - y) / y, with 1 / (a - e) <= (1 + 2 e / a) / a for
-        // e <= a / 2: the approximation against log at v, log's own error at both arguments,
-        // the argument's error
+        // eol's log form, eol(y) = -log(1 - y) / y, which both paths take when y - ey >= 1e-4 (the
+        // short form 1 + y / 2 of y < 1e-4, beyond ~4.3 standard deviations, is left to the exact
+        // path), with 1 / (a - e) <= (1 + 2 e / a) / a for e <= a / 2: the approximation against
+        // log at v, log's own error at both arguments, the argument's error
         const float v = F_(1.0) - fmin_(y, gxc::kOneMinus1e6);
         const float ev = ey + F_(2.0) * kU;
         const float lg = mlog(v);
         const float iv = mufu(v, 3), iy = mufu(y, 3);
         const float elg = __fmaf_rn(kLogRel + F_(5e-7), fabsf(lg), kLogAbs + F_(4e-7)) +
                           ev * iv * __fmaf_rn(F_(2.0) * ev, iv, F_(1.0)) * kSafe;
-        const float eo_l = -lg * iy;
-        const float eeo_l = __fmaf_rn(__fmaf_rn(fabsf(eo_l), ey, elg) * iy, __fmaf_rn(F_(2.0) * ey, iy, F_(1.0)) * kSafe,
-                                      F_(4e-7) * fabsf(eo_l));
-        const bool large = y - ey >= F_(1e-4) && ev <= F_(0.5) * v && ey <= F_(0.5) * y;
-        sure &= earg < F_(0.125) && (small || large);
-        const float eo = small ? eo_s : eo_l, de = (small ? eeo_s : eeo_l) * kSafe;
+        const float eo = -lg * iy;
+        const float eeo = __fmaf_rn(__fmaf_rn(fabsf(eo), ey, elg) * iy, __fmaf_rn(F_(2.0) * ey, iy, F_(1.0)) * kSafe,
+                                    F_(4e-7) * fabsf(eo));
+        sure &= earg < F_(0.125) && y - ey >= F_(1e-4) && ev <= F_(0.5) * v && ey <= F_(0.5) * y;
+        const float de = eeo * kSafe;
         // keep = clamp(eo / r1.y, 0, 1) against the exact draw, compared as u r1.y against eo
         const float ur = gx::next_u(&st) * r1.y;
         const bool reject = ur >= (eo + de) * (F_(1.0) + F_(6.0) * kU);
