@@ -42,10 +42,10 @@ typedef unsigned long long ull;
 // over every input they can get (gpsb_debug_fast_bounds); the exact maths' own errors are those
 // of fmath.h (exp 2 ulp, log 4 * 2^-24 relative or 2e-7 absolute).
 constexpr float kU = 6.0e-8f, kSafe = 1.01f;
-constexpr float kLogAbs = 7e-7f, kLogRel = 7e-7f;   // |mlog(v) - log(v)| <= kLogAbs + kLogRel |mlog(v)|, v in [kUMin, 1)
-constexpr float kSinCos = 2e-6f;                    // |msin/mcos(t) - sincos(t)|, t = RN(2 pi u), u = k 2^-24
+constexpr float kLogAbs = 3.5e-7f, kLogRel = 3.5e-7f;  // |mlog(v) - log(v)| <= kLogAbs + kLogRel |mlog(v)|, v in [kUMin, 1)
+constexpr float kSinCos = 1e-6f;                    // |msin/mcos(t) - sincos(t)|, t = RN(2 pi u), u = k 2^-24
 constexpr float kXMin = 1e-3f;                      // smallest x = -2 log u1 the bounds cover
-constexpr float kErMax = 4.6e-5f;                   // |r - r_exact| for x >= kXMin (r = x rsqrt(x))
+constexpr float kErMax = 2.5e-6f;                   // |r - r_exact| for x >= kXMin (r = x rsqrt(x))
 constexpr float kRMax = 5.77f;                      // largest r (u1 >= kUMin)
 constexpr float kEN = kErMax * (1.0f + 2.0f * kSinCos) + kRMax * (kSinCos + 2.01f * kU) + 1e-7f;  // one normal
 constexpr float kExpA = 6e-7f, kExpB = 1.5e-7f;     // |mexp(a) - exp(a)| <= (kExpA + kExpB |a|) mexp(a) + kExpTiny, a <= 0
