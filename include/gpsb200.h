@@ -203,7 +203,10 @@ gpsb_status gpsb_debug_fast_bounds(gpsb_renderer* r, float* ratios);
 gpsb_status gpsb_set_feature_accum(gpsb_renderer* r, float* feat_dev);
 
 /* ------------------------------------------------------------------- scene */
-/* GpsRenderer::set_gaussians (gps.rs:683). Host pointer. On error the old scene stays. */
+/* GpsRenderer::set_gaussians (gps.rs:683). Host pointer. On error the old scene stays. The new
+ * scene is staged in a second set of scene buffers that then swaps with the current one, so the
+ * renderer holds two scenes' worth of device memory after the first reload, and reloading a
+ * scene no larger than one it held before allocates nothing. */
 gpsb_status gpsb_set_gaussians(gpsb_renderer* r, const gpsb_gaussian* splats, size_t n);
 /* GpsRenderer::set_gaussians_sh (gps.rs:689-740): sh_rest holds 3*((d+1)^2-1) floats per
  * splat, channel-major (R.., G.., B..); sh_len must equal n*3*((d+1)^2-1) when degree >= 1. */
