@@ -761,7 +761,12 @@ __device__ __forceinline__ uint32_t emit_so(const FrameConst& f, const FTabs& T,
 
 constexpr int kPT = 256;               // threads per particle block
 constexpr uint32_t kRing = 64;         // per-warp ring of undecided PBVR particles (uint2 entries)
-constexpr uint32_t kFastGiveUp = 10;   // undecided lanes of one step above which a warp stops the fast test
+#ifndef GPSB_FAST_GIVE_UP
+#define GPSB_FAST_GIVE_UP 10
+#endif
+// undecided lanes of one step above which a warp stops the fast test for the rest of its tile
+// (measured on the bench views: 10 beats 4, 7, 16, 24 and never giving up)
+constexpr uint32_t kFastGiveUp = GPSB_FAST_GIVE_UP;
 static_assert(kTabFloats % 2 == 0, "the ring after the entry lists needs 8-byte alignment");
 
 // Largest j in [lo, hi) with off(j) <= v, by a 32-ary warp search (off(lo) <= v must hold).
