@@ -1,0 +1,38 @@
+"""Host-side helpers of bench.py (no GPU): the committed ncu figures it reads, the issue roofline it
+derives from them, the peak fallback and the workload description."""
+import os
+import sys
+from types import SimpleNamespace
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def test_committed_figures_parse():
+    assert bench.committed_traffic("k_particles") > 1e9
+    per = bench.committed_traffic("k_particles_warp_inst_per_particle")
+    assert per is not None and 5.0 < per < 40.0
+    assert bench.committed_traffic("no_such_kernel") is None
+
+
+def test_issue_roofline_arithmetic():
+    per = bench.committed_traffic("k_particles_warp_inst_per_particle")
+    st = SimpleNamespace(particles=7_000_000_000)
+    out = bench.issue_roofline(st, 100.0, 1, {"sm_mhz": 2000.0})
+    achieved = 7e9 / 0.1 * per
+    peak = 148 * 4 * 2000e6
+    assert abs(out["achieved"] - achieved) < 1e-6 * achieved and abs(out["peak"] - peak) < 1.0
+    assert abs(out["frac"] - achieved / peak) < 1e-12
+    # no clock samples or no particles: no estimate
+    assert bench.issue_roofline(st, 100.0, 1, {"sm_mhz": None}) is None
+    assert bench.issue_roofline(SimpleNamespace(particles=0), 100.0, 1, {"sm_mhz": 2000.0}) is None
+
+
+def test_peak_and_workload():
+    peak, kind = bench.measured_peak()
+    assert peak > 1000.0 and kind in ("of measured", "of fallback")
+    cfg = bench.workload_config()
+    assert cfg["gaussians"] == bench.N_SPLATS and cfg["resolution"] == [bench.W, bench.H]
+    assert cfg["views"] == [v for v, _ in bench.VIEWS] and cfg["ensembles_per_view"] == bench.ENS
