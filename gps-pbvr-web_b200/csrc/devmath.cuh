@@ -147,7 +147,7 @@ __device__ __forceinline__ float mix_(float a, float b, float t) { return a * (F
 // corrected_radius_lut (gps_splat.wgsl:117-130) with the o-row (i0, a) hoisted per splat
 __device__ __forceinline__ float corrected_radius_lut(const float* lut, uint32_t i0, float a, float u,
                                                      const float* lg = gx::tab_log()) {
-    float v = -gx::log_t(fmax_(F_(1.0) - u, gxc::kUMin), lg);
+    float v = -gx::log_t_pos(fmax_(F_(1.0) - u, gxc::kUMin), lg);
     float fv = fmin_(sqrt_(v) * gxc::kLutFv, F_(128.0));
     uint32_t j0 = min(f2u(fv), 127u);
     float b = fv - (float)j0;
@@ -190,7 +190,7 @@ __device__ inline float pixel_density_scale(const FrameConst& f, float depth) {
 }
 __device__ __forceinline__ float eol(float x, const float* lg = gx::tab_log()) {
     if (x < F_(1e-4)) return F_(1.0) + F_(0.5) * x;
-    return div_(-gx::log_t(F_(1.0) - fmin_(x, gxc::kOneMinus1e6), lg), x);
+    return div_(-gx::log_t_pos(F_(1.0) - fmin_(x, gxc::kOneMinus1e6), lg), x);  // argument >= 1e-6
 }
 
 // splat_colour (gps_splat.wgsl:210-251)

@@ -208,6 +208,24 @@ GX_HD float log_t(float x, const float* T) {
     return fma_(ef, kLn2Hi, thi) + (fma_(ef, kLn2Lo, tlo) + p);
 }
 GX_HD float log(float x) { return log_t(x, tab_log()); }
+// log_t for arguments known to be positive and normal (>= 2^-126, finite): the same arithmetic
+// without the special-value test, so the same result bit for bit.
+GX_HD float log_t_pos(float x, const float* T) {
+    const uint32_t b = f2b(x);
+    const uint32_t mb = b & 0x007FFFFFu;
+    const uint32_t big = mb >= 0x00400000u ? 1u : 0u;
+    const int e = (int)(b >> 23) - 127 + (int)big;
+    const float m = b2f(mb | (big ? 0x3F000000u : 0x3F800000u));
+    const int i = (int)rint_((m - 1.0f) * 128.0f);
+    float rinv, thi, tlo, pad;
+    ld4(T, i + 32, &rinv, &thi, &tlo, &pad);
+    const float t = fma_(m, rinv, -1.0f);
+    float q = fma_(t, -0.25f, 3.33333343e-1f);
+    q = fma_(t, q, -0.5f);
+    const float p = fma_(t * t, q, t);
+    const float ef = (float)e;
+    return fma_(ef, kLn2Hi, thi) + (fma_(ef, kLn2Lo, tlo) + p);
+}
 
 // sin and cos of x together; accurate for |x| < 1e4 (the renderer's angles are 2 pi U).
 GX_HD void sincos_t(float x, const float* T, float* s, float* c) {

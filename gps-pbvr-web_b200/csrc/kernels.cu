@@ -518,7 +518,7 @@ struct Normal {
         if (has) { has = false; return spare; }
         float u1 = fmax_(gx::next_u(st), gxc::kUMin);
         float u2 = gx::next_u(st);
-        float r = sqrt_(-F_(2.0) * gx::log_t(u1, T.lg));
+        float r = sqrt_(-F_(2.0) * gx::log_t_pos(u1, T.lg));  // u1 >= kUMin
         float sn, cs;
         gx::sincos_t(gxc::kTwoPi * u2, T.sc, &sn, &cs);
         spare = r * sn;
