@@ -1056,10 +1056,14 @@ static void launch_particles_t(const FrameConst& fc, const float4* rec, const fl
     size_t smem = (kTabFloats + 2 * ((size_t)E + 1) + 2 * (kPT * IPT + 2)) * sizeof(uint32_t);
     if (MC == 0 && !fc.exact_radius) smem += kLutN * sizeof(float);
     if (MC == 1 && FM == 1) smem += (size_t)(kPT / 32) * kRing * sizeof(uint2);
-    static size_t attr = 0;
-    if (smem > 48 * 1024 && smem > attr) {
+    // the attribute belongs to each device's context: remember the size set per device ordinal
+    static size_t attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const bool known = dev >= 0 && dev < 64;
+    if (smem > 48 * 1024 && (!known || smem > attr[dev])) {
         cudaFuncSetAttribute(k_particles<MC, IPT, FM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = smem;
+        if (known) attr[dev] = smem;
     }
     k_particles<MC, IPT, FM><<<grid, kPT, smem, st>>>(fc, rec, lut, clist, etot, first_seed, E, sub, unit_counter, stats);
 }
