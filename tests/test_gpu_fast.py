@@ -96,3 +96,25 @@ def test_fast_decisions_near_view_mostly_decided(scene):
     # the near view writes few of its particles: the fast decisions settle most of the rest
     assert mismatch == 0 and st.points > 0 and st.subpixel_writes < 0.05 * st.particles
     assert undecided < 0.4 * st.particles, (undecided, st.particles, st.subpixel_writes)
+
+
+def test_fast_decisions_bench_scene_validated():
+    """The 560k-Gaussian benchmark scene at 1280x720 (near / mid / far orbit views, 2 ensembles each):
+    every particle's fast answer agrees with the exact path, and the images match bit for bit."""
+    from gps_pbvr_web_b200 import scenes
+    splats, sh, deg = PKG.load_ply(scenes.cluster_scene(560_000, seed=0, degree=3))
+    w, h = 1280, 720
+    r = PKG.GpsRenderer(w, h, 1)
+    r.set_gaussians_sh(splats, sh, deg)
+    p = params(CASES[0])
+    total = 0
+    for d in (2.5, 7.0, 20.0):
+        cam = PKG.OrbitCamera(target=(0.0, 0.0, 0.0), distance=d, yaw=0.6, pitch=0.25, up=(0.0, -1.0, 0.0),
+                              fov_y=0.9).to_camera(w, h)
+        a2, s2, (_, mismatch) = render(r, cam, p, 2, ens=2, seed=3)
+        a1, s1, _ = render(r, cam, p, 1, ens=2, seed=3)
+        assert mismatch == 0, (d, mismatch)
+        assert np.array_equal(a1.view(np.uint32), a2.view(np.uint32)) and s1.counters() == s2.counters()
+        total += s2.particles
+    assert total > 3e9 and r.debug_error_word() == 0
+    r.close()
