@@ -3,8 +3,9 @@
 //   k_sp_project    sp_project (gps_splat.wgsl:737-777): 24-bit far-to-near key, quad record,
 //                   GPS demand probe, plus the screen-tile rectangle of the splat.
 //   radix_sort_pairs  stable LSD onesweep sort (replaces gps_sort.wgsl): one histogram pass for
-//                   all digits, then one kernel per digit that ranks keys with warp-match
-//                   (__match_any_sync), resolves tile offsets by a decoupled lookback per digit and
+//                   all digits, then one kernel per digit that ranks keys within each warp by
+//                   peer groups (one ballot per digit bit), resolves tile offsets by a decoupled
+//                   lookback per digit and
 //                   scatters. Digit width 4, 6 or 8 bits.
 //   tile binning    (tile id, sorted rank) entries, stably sorted by tile, give every screen tile its
 //                   splats in depth order.
