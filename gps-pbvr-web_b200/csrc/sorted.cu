@@ -5,8 +5,7 @@
 //   radix_sort_pairs  stable LSD onesweep sort (replaces gps_sort.wgsl): one histogram pass for
 //                   all digits, then one kernel per digit that ranks keys within each warp by
 //                   peer groups (one ballot per digit bit), resolves tile offsets by a decoupled
-//                   lookback per digit and
-//                   scatters. Digit width 4, 6 or 8 bits.
+//                   lookback per digit and scatters. Digit width 4, 6 or 8 bits.
 //   tile binning    (tile id, sorted rank) entries, stably sorted by tile, give every screen tile its
 //                   splats in depth order.
 //   k_blend         one block per tile, front-to-back f32 blending with early termination
