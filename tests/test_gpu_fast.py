@@ -118,3 +118,29 @@ def test_fast_decisions_bench_scene_validated():
         total += s2.particles
     assert total > 3e9 and r.debug_error_word() == 0
     r.close()
+
+
+def test_scene_reloads_reuse_buffers_and_match_fresh_renderers():
+    """Reloading scenes of different sizes into one renderer (the spare scene buffers swap, the
+    per-ensemble buffers grow) renders exactly what a fresh renderer renders."""
+    from gps_pbvr_web_b200 import scenes
+    small = PKG.load_ply(scenes.cluster_scene(20_000, seed=5, degree=1))
+    large = PKG.load_ply(scenes.cluster_scene(120_000, seed=6, degree=3))
+    _, cam = cams()[1]
+    p = params(CASES[0])
+
+    def fresh(sc):
+        r = PKG.GpsRenderer(W, H, 1)
+        r.set_gaussians_sh(*sc)
+        out = render(r, cam, p, 1, ens=2, seed=9)[0]
+        r.close()
+        return out
+
+    want_small, want_large = fresh(small), fresh(large)
+    r = PKG.GpsRenderer(W, H, 1)
+    for sc, want in ((small, want_small), (large, want_large), (small, want_small), (large, want_large)):
+        r.set_gaussians_sh(*sc)
+        got = render(r, cam, p, 1, ens=2, seed=9)[0]
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert r.debug_error_word() == 0
+    r.close()
