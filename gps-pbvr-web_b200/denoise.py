@@ -116,6 +116,13 @@ class Denoiser:
             q["b"].copy_(sd[n]["b"])
         self.sync_weights()
 
+    def reset_optimizer(self):
+        """Zeroes Adam's moments and step count (after restoring earlier weights)."""
+        for q in self.p.values():
+            for k in ("mw", "vw", "mb", "vb"):
+                q[k].zero_()
+        self.t = 0
+
     def param_count(self):
         return sum(q["cout"] * 9 * c_real + q["cout"] for (n, _, c_real, _), q in zip(LAYERS, self.p.values()))
 

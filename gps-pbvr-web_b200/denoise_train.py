@@ -135,8 +135,33 @@ def make_frames(pkg, fr, scene_specs, cams_per_scene, in_ens, tgt_ens, rng, seed
     return torch.stack(xs), torch.stack(bases), torch.stack(tgts), meta
 
 
-def train(net, x, base, target, steps, batch, crop, lr, rng, log_every=100):
-    """Adam on random crop batches; returns (loss history, ms per step)."""
+class CollapseGuard:
+    """Watches the logged training loss. Adam at a high rate can throw this network into a state
+    it does not leave (a 10,000-step run at lr 1e-3 jumped from 0.022 to 0.09 at step ~2,400 and
+    stayed there, its output no better than the input); when a logged loss exceeds `factor` times
+    the best one seen after `warmup` logs, the guard restores the weights of that best log,
+    clears the optimiser state and halves the rate scale it returns."""
+
+    def __init__(self, factor=3.0, warmup=5):
+        self.factor, self.warmup = factor, warmup
+        self.best, self.snap, self.logs, self.scale, self.restores = float("inf"), None, 0, 1.0, []
+
+    def check(self, step, loss, net):
+        """Called at every logged step; returns the learning-rate scale for the steps that follow."""
+        self.logs += 1
+        if self.snap is not None and self.logs > self.warmup and loss > self.factor * self.best:
+            net.load_state_dict(self.snap)
+            net.reset_optimizer()
+            self.scale *= 0.5
+            self.restores.append((step, loss, self.best))
+        elif loss < self.best:
+            self.best, self.snap = loss, net.state_dict()
+        return self.scale
+
+
+def train(net, x, base, target, steps, batch, crop, lr, rng, log_every=100, guard=None):
+    """Adam on random crop batches (cosine decay, with a CollapseGuard); returns (loss history,
+    ms per step). The guard's restores are in guard.restores."""
     import torch
     from gps_pbvr_web_b200 import denoise as dn
     N, H, W, _ = x.shape
@@ -145,6 +170,8 @@ def train(net, x, base, target, steps, batch, crop, lr, rng, log_every=100):
     tb = torch.zeros(batch, crop, crop, 3, device="cuda")
     crops = torch.zeros(batch, 3, dtype=torch.int32, device="cuda")
     hist = []
+    guard = guard if guard is not None else CollapseGuard()
+    scale = 1.0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for s in range(steps):
@@ -152,10 +179,11 @@ def train(net, x, base, target, steps, batch, crop, lr, rng, log_every=100):
                       rng.integers(0, W - crop + 1, batch)], axis=1).astype(np.int32)
         crops.copy_(torch.from_numpy(c))
         dn.crop(x, base, target, crops, crop, crop, xb, bb, tb, err=net.err)
-        step_lr = lr * (0.5 * (1 + math.cos(math.pi * s / steps)))  # cosine decay
+        step_lr = scale * lr * (0.5 * (1 + math.cos(math.pi * s / steps)))  # cosine decay
         loss = net.train_step(xb, bb, tb, lr=step_lr)
         if s % log_every == 0 or s == steps - 1:
             hist.append((s, float(loss.item())))
+            scale = guard.check(s, hist[-1][1], net)
     torch.cuda.synchronize()
     return hist, (time.perf_counter() - t0) * 1e3 / steps
 
@@ -301,7 +329,8 @@ def main(argv=None):
         gate_limit = dn.load_weights(net, args.load)
         hist, ms_step = [], 0.0
     else:
-        hist, ms_step = train(net, x, base, target, args.steps, args.batch, args.crop, args.lr, rng)
+        guard = CollapseGuard()
+        hist, ms_step = train(net, x, base, target, args.steps, args.batch, args.crop, args.lr, rng, guard=guard)
         gate_limit = 1.5 * float(x[..., 5].float().mean(dim=(1, 2)).max())
     del x, base, target
     torch.cuda.empty_cache()
@@ -309,6 +338,7 @@ def main(argv=None):
                     [4, 8, 16, 32, 64, 128], rng, 7_000_000, gate_limit)
     save_weights(net, args.weights, gate_limit)
     res = {"config": vars(args), "train_frames": len(meta), "data_seconds": t_data, "loss_history": hist,
+           "guard_restores": [] if args.load else guard.restores,
            "ms_per_train_step": ms_step, "params": net.param_count(), "gate_limit": gate_limit,
            "error_word": net.error_word(), "eval": rows}
     with open(args.out, "w") as f:
