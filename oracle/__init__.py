@@ -50,6 +50,7 @@ def _declare(L):
         ("o2_render_sorted", C.c_int, [P, U32, P, U32, P, U32, U32, U32, P, P, P, P, P, P]),
         ("o2_composite", C.c_int, [P, U32, U32, C.c_float, U32, U32, U32, P]),
         ("o2_fmath_eval", None, [C.c_int, P, P, SZ]),
+        ("o2_fast_check", C.c_int, [P, U32, P, U32, P, U32, U32, U32, P, P, U32, U32, U32, C.c_int, P]),
     ]:
         f = getattr(L, name)
         f.restype = res
@@ -213,6 +214,22 @@ def o2_render_ensembles(splats, sh, sh_degree, lut, w, h, spp_side, cam17, param
                               ctypes.cast(ctypes.pointer(params), C.c_void_p), first_seed, count, _p(acc), _p(st),
                               _p(counts), _p(packed))
     return acc, st, counts, packed
+
+
+def o2_fast_check(splats, sh, sh_degree, lut, w, h, spp_side, cam17, params, first_seed, count, perturb_seed=0,
+                  mode=0):
+    """The renderer's PBVR fast decisions restated with every approximation pushed to the edge of
+    its assumed error bound (mode 0 random signs, 1 all +, 2 all -), against the exact path over
+    every particle: returns (particles, decided, decided wrongly, points)."""
+    import ctypes
+    g, s = _o2_scene(splats, sh)
+    out = np.zeros(4, np.uint64)
+    rc = lib().o2_fast_check(_p(g), g.shape[0], _p(s), sh_degree, _p(np.ascontiguousarray(lut, np.float32)), w, h,
+                             spp_side, _p(_f64(cam17, 17)), ctypes.cast(ctypes.pointer(params), C.c_void_p),
+                             first_seed, count, perturb_seed, mode, _p(out))
+    if rc != 0:
+        raise ValueError("o2_fast_check: PBVR methods only")
+    return tuple(int(v) for v in out)
 
 
 def o2_render_sorted(splats, sh, sh_degree, lut, w, h, spp_side, cam17, params):

@@ -26,6 +26,7 @@
 #include <math.h>
 #include <vector>
 #include <algorithm>
+#include <cmath>
 
 #include "../include/gpsb200.h"
 #include "../gps-pbvr-web_b200/csrc/fmath.h"
@@ -379,19 +380,20 @@ struct Pipeline {
         cb = {l20, l21, l22};
     }
 
-    // emit_particle_pbvr (gps_splat.wgsl:490-532)
-    void emit_pbvr(uint32_t gid, Rng& rng, V4 a, V4 b, V4 c, V4 d, V3 ca, V3 cb) {
+    // emit_particle_pbvr (gps_splat.wgsl:490-532): the answer of particle `rng`, 0 = not a point,
+    // 1 = a point off screen, 3 = a point written to subpixel idx at depth_z
+    uint32_t pbvr_eval(Rng& rng, V4 a, V4 b, V4 c, V4 d, V3 ca, V3 cb, uint32_t& idx, float& depth_z) {
         rng.has_spare = false;
         float uz = rng.normal();
         float uy = rng.normal();
         float ux = rng.normal();
         if (f.pbvr[0] == 3u) {
-            if (rng.next() >= b.w) return;
+            if (rng.next() >= b.w) return 0u;
         }
         V3 world = {c.x + ca.x * ux, c.y + (ca.y * ux + ca.z * uy), c.z + (cb.x * ux + cb.y * uy + cb.z * uz)};
         V3 p = sub3(world, xyz(f.pos));
         V3 cam = {dot3(xyz(f.rot0), p), dot3(xyz(f.rot1), p), dot3(xyz(f.rot2), p)};
-        if (cam.z <= f.prm.y) return;
+        if (cam.z <= f.prm.y) return 0u;
         float pix_x = gx::div_(f.intr.x * cam.x, cam.z) + f.intr.z;
         float pix_y = gx::div_(f.intr.y * cam.y, cam.z) + f.intr.w;
         uint32_t flags = f.pbvr[2];
@@ -405,16 +407,23 @@ struct Pipeline {
         if (flags & 1u) {
             float dvx = pix_x - a.x, dvy = pix_y - a.y;
             float r2 = c.w * dvx * dvx + (float)2.0 * d.x * dvx * dvy + d.y * dvy * dvy;
-            if (rng.next() >= radial_keep(a.w, r2)) return;
+            if (rng.next() >= radial_keep(a.w, r2)) return 0u;
         }
-        float depth_z = cam.z;
+        depth_z = cam.z;
         if (flags & 2u) depth_z = a.z;
-        st.c[0] += 1;  // points (depth pass only)
-        if (pix_x < (float)0.0 || pix_x >= (float)W || pix_y < (float)0.0 || pix_y >= (float)H) return;
+        if (pix_x < (float)0.0 || pix_x >= (float)W || pix_y < (float)0.0 || pix_y >= (float)H) return 1u;
         uint32_t px = gx::f2u(pix_x), py = gx::f2u(pix_y);
         uint32_t sx = std::min(side - 1u, gx::f2u((pix_x - (float)px) * (float)side));
         uint32_t sy = std::min(side - 1u, gx::f2u((pix_y - (float)py) * (float)side));
-        write((py * W + px) * S + sy * side + sx, depth_z, gid);
+        idx = (py * W + px) * S + sy * side + sx;
+        return 3u;
+    }
+    void emit_pbvr(uint32_t gid, Rng& rng, V4 a, V4 b, V4 c, V4 d, V3 ca, V3 cb) {
+        uint32_t idx = 0;
+        float depth_z = (float)0.0;
+        const uint32_t r = pbvr_eval(rng, a, b, c, d, ca, cb, idx, depth_z);
+        if (r & 1u) st.c[0] += 1;  // points (depth pass only)
+        if (r == 3u) write(idx, depth_z, gid);
     }
 
     uint32_t prepare_gps(uint32_t i, const Proj& pr, float o) {
@@ -565,6 +574,161 @@ struct Pipeline {
     }
 };
 
+
+// ----------------------------------------------------------------------- fast-decision check
+// A restatement of the renderer's PBVR fast decisions (pbvr_fast, fast_pair and fast_bounds_of in
+// gps-pbvr-web_b200/csrc/kernels.cu, line for line) in which every hardware approximation is
+// replaced by the exact value pushed to the edge of the error bound the decisions assume:
+// log by +-(kLogAbs + kLogRel |log|), the Box-Muller radius by +-kErMax, sin and cos by
+// +-kSinCos, exp by a relative +-(kExpA + kExpB |a|), reciprocals by +-2^-23 relative (signs
+// random per operand, or all + / all -). Whenever the restated fast path answers "not a point"
+// or "a point off screen", the exact path (pbvr_eval) must agree: this checks the error
+// propagation of the decisions on the CPU, independently of the device's approximations (whose
+// constants the renderer checks exhaustively on the GPU).
+namespace fastcheck {
+constexpr float kU = 6.0e-8f, kSafe = 1.01f;
+constexpr float kLogAbs = 3.5e-7f, kLogRel = 3.5e-7f, kSinCos = 1e-6f, kXMin = 1e-3f, kErMax = 2.5e-6f;
+constexpr float kRMax = 5.77f;
+constexpr float kEN = kErMax * (1.0f + 2.0f * kSinCos) + kRMax * (kSinCos + 2.01f * kU) + 1e-7f;
+constexpr float kExpA = 6e-7f, kExpB = 1.5e-7f, kExpTiny = 1.5e-38f;
+constexpr float kEdge = 0.999f;  // how far to the edge of each bound the perturbations go
+
+struct Perturb {
+    uint32_t st;
+    int mode;  // 0 random signs, 1 all +, 2 all -
+    float sgn() {
+        if (mode == 1) return 1.0f;
+        if (mode == 2) return -1.0f;
+        st = gx::pcg(st);
+        return (st >> 16) & 1u ? 1.0f : -1.0f;
+    }
+    float log_(float v) {
+        const float e = gx::log(v);
+        return e + sgn() * (kLogAbs + kLogRel * fabsf(e)) * kEdge;
+    }
+    float exp_(float a) {
+        const double e = (double)gx::exp(a);
+        return (float)(e * (1.0 + sgn() * (kExpA + kExpB * fabs((double)a)) * kEdge));
+    }
+    float rcp_(float x) { return (float)((1.0 / (double)x) * (1.0 + sgn() * 1.19e-7 * kEdge)); }
+};
+
+struct Bounds { float fx_ecx, fy_ecy, ecz, kq, gx_, gy_; };
+
+// fast_bounds_of
+static Bounds bounds_of(const Frame& f, V3 g0, V3 ca, V3 cb, float a, float b, float c) {
+    const float sx = fabsf(ca.x), sy = fabsf(ca.y) + fabsf(ca.z), sz = fabsf(cb.x) + fabsf(cb.y) + fabsf(cb.z);
+    const float gm = kRMax + kEN;
+    const float Mx = fabsf(g0.x) + fabsf(f.pos.x) + sx * gm, My = fabsf(g0.y) + fabsf(f.pos.y) + sy * gm,
+                Mz = fabsf(g0.z) + fabsf(f.pos.z) + sz * gm;
+    const float ex = sx * kEN + 6.0f * kU * Mx, ey = sy * kEN + 10.0f * kU * My, ez = sz * kEN + 14.0f * kU * Mz;
+    auto row = [&](V4 q) {
+        const float ax = fabsf(q.x), ay = fabsf(q.y), az = fabsf(q.z);
+        return (ax * ex + ay * ey + az * ez + 10.0f * kU * (ax * (Mx + ex) + ay * (My + ey) + az * (Mz + ez))) * 1.02f;
+    };
+    const float ecx = row(f.rot0), ecy = row(f.rot1), ecz = row(f.rot2);
+    Bounds B;
+    B.fx_ecx = fabsf(f.intr.x) * ecx * 1.02f;
+    B.fy_ecy = fabsf(f.intr.y) * ecy * 1.02f;
+    B.ecz = ecz * kSafe;
+    B.kq = (fabsf(a) + 2.0f * fabsf(b) + fabsf(c)) * 1.02f;
+    B.gx_ = 2.0f * (fabsf(a) + fabsf(b)) * 1.02f;
+    B.gy_ = 2.0f * (fabsf(b) + fabsf(c)) * 1.02f;
+    if (!std::isfinite(ecx) || !std::isfinite(ecy) || !std::isfinite(ecz) || !std::isfinite(B.kq))
+        B.fx_ecx = B.fy_ecy = B.ecz = B.kq = B.gx_ = B.gy_ = INFINITY;
+    return B;
+}
+
+// fast_pair: exact draws, approximated radius and angle functions
+static bool pair(uint32_t& st, Perturb& pt, float& c, float& s) {
+    const float u1 = fmax_(gx::next_u(&st), gxc::kUMin);
+    const float u2 = gx::next_u(&st);
+    const float le = gx::log(u1);
+    const float x = -2.0f * pt.log_(u1);
+    const float re = gx::sqrt_(-2.0f * le);
+    const float r = fmaxf(re + pt.sgn() * kErMax * kEdge, 0.0f);
+    float se, ce;
+    gx::sincos(gxc::kTwoPi * u2, &se, &ce);
+    c = r * (ce + pt.sgn() * kSinCos * kEdge);
+    s = r * (se + pt.sgn() * kSinCos * kEdge);
+    return x >= kXMin;
+}
+
+// pbvr_fast; R as the renderer's record: r0 (mean xy, depth, o), r1 (keep, eol(o), |fx| ecx,
+// |fy| ecy), r2 (centre, a), r3 (b, c, ecz, K), r4 (l00, l10, l11, G_x), r5 (l20, l21, l22, G_y)
+static uint32_t fast(const Frame& f, uint32_t W, uint32_t H, uint32_t st, const V4* R, Perturb& pt) {
+    float uz, uy, ux, jy;
+    bool ok = pair(st, pt, uz, uy);
+    ok &= pair(st, pt, ux, jy);
+    const V4 r1 = R[1];
+    if (f.pbvr[0] == 3u) {
+        if (gx::next_u(&st) >= r1.x) return 0u;
+    }
+    const V4 r2 = R[2], r3 = R[3], r4 = R[4], r5 = R[5];
+    const float px = fmaf(r4.x, ux, r2.x) - f.pos.x;
+    const float py = fmaf(r4.z, uy, fmaf(r4.y, ux, r2.y)) - f.pos.y;
+    const float pz = fmaf(r5.z, uz, fmaf(r5.y, uy, fmaf(r5.x, ux, r2.z))) - f.pos.z;
+    const float cz = fmaf(f.rot2.z, pz, fmaf(f.rot2.y, py, f.rot2.x * px));
+    const float ecz = r3.z;
+    const bool behind = cz + ecz <= f.prm.y;
+    const float czl = cz - ecz;
+    bool sure = czl > f.prm.y && czl > 3.0f * ecz && cz < 1e30f && czl > 1e-6f;
+    const float cx = fmaf(f.rot0.z, pz, fmaf(f.rot0.y, py, f.rot0.x * px));
+    const float cy = fmaf(f.rot1.z, pz, fmaf(f.rot1.y, py, f.rot1.x * px));
+    const float icz = pt.rcp_(cz);
+    const float icl = icz * fmaf((2.0f * kSafe) * ecz, icz, kSafe);
+    const float kt = fmaf(ecz, icl, 1e-6f + 2.0f * kU);
+    const float tx = (f.intr.x * cx) * icz, ty = (f.intr.y * cy) * icz;
+    float pix_x = tx + f.intr.z, pix_y = ty + f.intr.w;
+    float epx = fmaf(fabsf(tx), kt, fmaf(r1.z, icl, 2.0f * kU * fabsf(f.intr.z)));
+    float epy = fmaf(fabsf(ty), kt, fmaf(r1.w, icl, 2.0f * kU * fabsf(f.intr.w)));
+    const uint32_t flags = f.pbvr[2];
+    if (flags & 4u) {
+        float jx, js;
+        sure &= pair(st, pt, jx, js);
+        const float sd = gx::sqrt_(fmax_(f.pos.w, 0.0f));
+        const float kj = fabsf(sd) * (kEN + 4.0f * kU * kRMax);
+        pix_x = pix_x + sd * jx;
+        pix_y = pix_y + sd * jy;
+        epx = fmaf(4.0f * kU, fabsf(pix_x), epx + kj);
+        epy = fmaf(4.0f * kU, fabsf(pix_y), epy + kj);
+    }
+    sure &= fabsf(pix_x) < 1e30f && fabsf(pix_y) < 1e30f && epx < 1e30f && epy < 1e30f;
+    const float mx = kSafe * epx, my = kSafe * epy;
+    const bool off = pix_x + mx < 0.0f || pix_x - mx >= (float)W || pix_y + my < 0.0f || pix_y - my >= (float)H;
+    uint32_t res = off ? 1u : 2u;
+    if (flags & 1u) {
+        const V4 r0 = R[0];
+        const float dvx = pix_x - r0.x, dvy = pix_y - r0.y;
+        const float e = fmaxf(fmaf(2.0f * kU, fabsf(pix_x) + fabsf(r0.x), epx), fmaf(2.0f * kU, fabsf(pix_y) + fabsf(r0.y), epy));
+        const float dx2 = dvx * dvx, dy2 = dvy * dvy;
+        const float r2v = fmaf(r2.w, dx2, fmaf(2.0f * r3.x, dvx * dvy, r3.y * dy2));
+        const float m2 = fmaf(r4.w, dx2, r5.w * dy2);
+        const float er2 = fmaf(fmaf(r4.w, fabsf(dvx), r5.w * fabsf(dvy)), e, fmaf(r3.w * e, e, 10.0f * kU * m2));
+        const float a2 = fmaxf(r2v, 0.0f);
+        const float earg = er2 * (0.5f * kSafe);
+        const float oo = fmin_(r0.w, gxc::kOneMinus1e6);
+        const float y = oo * pt.exp_(-0.5f * a2);
+        const float rel = fmaf(earg, 1.0f + earg, fmaf(0.5f * kExpB, a2, kExpA + 5.4e-7f + 2.0f * kU));
+        const float ey = fmaf(y, rel * (1.25f * kSafe), 2.02f * kExpTiny);
+        const float v = 1.0f - fmin_(y, gxc::kOneMinus1e6);
+        const float ev = ey + 2.0f * kU;
+        const float lg = pt.log_(v);
+        const float iv = pt.rcp_(v), iy = pt.rcp_(y);
+        const float elg = fmaf(kLogRel + 5e-7f, fabsf(lg), kLogAbs + 4e-7f) + ev * iv * fmaf(2.0f * ev, iv, 1.0f) * kSafe;
+        const float eo = -lg * iy;
+        const float eeo = fmaf(fmaf(fabsf(eo), ey, elg) * iy, fmaf(2.0f * ey, iy, 1.0f) * kSafe, 4e-7f * fabsf(eo));
+        sure &= earg < 0.125f && y - ey >= 1e-4f && ev <= 0.5f * v && ey <= 0.5f * y;
+        const float de = eeo * kSafe;
+        const float ur = gx::next_u(&st) * r1.y;
+        const bool reject = ur >= (eo + de) * (1.0f + 6.0f * kU);
+        const bool keep = ur * (1.0f + 6.0f * kU) < eo - de;
+        res = reject ? 0u : (keep ? res : 2u);
+    }
+    res = behind ? 0u : (sure ? res : 2u);
+    return ok ? res : 2u;
+}
+}  // namespace fastcheck
 }  // namespace o2
 
 // ============================================================================ C entry points
@@ -805,6 +969,58 @@ int o2_composite(const float* accum, uint32_t W, uint32_t H, float exposure, uin
 }
 
 // Shared-function probes for the fmath tests: out[i] = f(in[i]) for f in {exp, log, sin, cos}.
+// The fast-decision check (fastcheck above) over every particle of `count` ensembles of a PBVR
+// frame: out[0] particles, out[1] decided by the restated fast path, out[2] decided wrongly,
+// out[3] points among the particles. mode: 0 random perturbation signs (seeded by perturb_seed),
+// 1 all +, 2 all -.
+int o2_fast_check(const gpsb_gaussian* g, uint32_t n, const float* sh, uint32_t sh_degree, const float* lut,
+                  uint32_t W, uint32_t H, uint32_t side, const gpsb_camera* cam, const gpsb_params* prm,
+                  uint32_t first_seed, uint32_t count, uint32_t perturb_seed, int mode, uint64_t* out) {
+    side = std::max(1u, std::min(side, 4u));
+    if (prm->method == GPSB_METHOD_GPS || prm->method == GPSB_METHOD_SCREEN_OCCUPANCY) return -1;
+    Scene s = make_scene(g, n, sh, sh_degree, lut);
+    Stats st;
+    memset(&st, 0, sizeof st);
+    fastcheck::Perturb pt{perturb_seed * 2654435761u + 1u, mode};
+    for (int k = 0; k < 4; ++k) out[k] = 0;
+    for (uint32_t e = 0; e < count; ++e) {
+        Pipeline pl(s, st);
+        pl.f = make_frame(s, *cam, *prm, W, H, side, first_seed + e);
+        pl.W = W; pl.H = H; pl.side = side; pl.S = side * side;
+        pl.proj.assign((size_t)n * 6u, V4{0, 0, 0, 0});
+        pl.running = 0;
+        pl.overflow = false;
+        std::vector<uint32_t> cnt(n);
+        for (uint32_t i = 0; i < n; ++i) cnt[i] = pl.prepare(i);
+        if (pl.overflow) continue;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (!cnt[i]) continue;
+            const V4* P = &pl.proj[(size_t)i * 6u];
+            const V4 a = P[0], b = P[1], c = P[2], d = P[3], e4 = P[4], f4 = P[5];
+            const V3 ca = {e4.x, e4.y, e4.z}, cb = {f4.x, f4.y, f4.z};
+            const fastcheck::Bounds B = fastcheck::bounds_of(pl.f, {c.x, c.y, c.z}, ca, cb, c.w, d.x, d.y);
+            const float h = Pipeline::eol(fmin_(a.w, gxc::kOneMinus1e6));
+            const V4 R[6] = {a, {b.w, h, B.fx_ecx, B.fy_ecy}, c, {d.x, d.y, B.ecz, B.kq},
+                             {ca.x, ca.y, ca.z, B.gx_}, {cb.x, cb.y, cb.z, B.gy_}};
+            for (uint32_t k = 0; k < cnt[i]; ++k) {
+                const uint32_t seed = gx::particle_seed(i, k + 1u, pl.f.cfg[0]);
+                Rng rng{seed, false, (float)0.0};
+                uint32_t idx;
+                float dz;
+                const uint32_t exact = pl.pbvr_eval(rng, a, b, c, d, ca, cb, idx, dz);
+                const uint32_t q = fastcheck::fast(pl.f, W, H, seed, R, pt);
+                out[0] += 1;
+                out[3] += exact & 1u;
+                if (q != 2u) {
+                    out[1] += 1;
+                    out[2] += q != exact ? 1u : 0u;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
 void o2_fmath_eval(int which, const float* in, float* out, size_t n) {
     for (size_t i = 0; i < n; ++i) {
         float x = in[i];
