@@ -290,13 +290,15 @@ def micro_scan_sort(pkg, r, stream, peak):
     return out
 
 
-def denoise_measure(pkg, r, stream, cams, p, per_view_ms, ref_ens=256):
+def denoise_measure(pkg, r, stream, cams, p, per_view_ms, ref_ens=256, w=None, h=None,
+                    counts=(4, 8, 16, 32, 64, 128)):
     """The "ms to PSNR vs the 256-ensemble reference: denoised batch vs plain" comparison, per view:
     the 4-ensemble frame through the trained denoiser (committed weights) against the plain
     accumulation. PSNR (peak 1, linear RGB clamped to [0, 1]) against a 256-ensemble reference with
     disjoint seeds; the plain path's PSNR is measured at 4..128 ensembles and the ensembles it
     needs to match the denoised PSNR come from its fitted error model MSE(N) = s2 (1/N + 1/256);
-    times are ensembles x the view's ms per ensemble of this run, plus the denoiser's GPU time."""
+    times are ensembles x the view's ms per ensemble of this run, plus the denoiser's GPU time.
+    w, h: the renderer's size (default the benchmark's); counts: the plain ensemble counts measured."""
     import torch
     from gps_pbvr_web_b200 import denoise as dn
     from gps_pbvr_web_b200 import denoise_train as T
@@ -304,7 +306,8 @@ def denoise_measure(pkg, r, stream, cams, p, per_view_ms, ref_ens=256):
     gate = dn.load_weights(net)
     out = {"weights": "gps-pbvr-web_b200/weights/denoiser_pbvr_c3r.npz", "reference_ensembles": ref_ens,
            "input_ensembles": 4, "views": {}}
-    P = W * H
+    w, h = w or W, h or H
+    P = w * h
     with torch.cuda.stream(stream):
         for name, cam in cams:
             r.reset_accum()
@@ -320,16 +323,16 @@ def denoise_measure(pkg, r, stream, cams, p, per_view_ms, ref_ens=256):
             base = torch.zeros(P, 3, device="cuda")
             dn.pack(acc, feat, x, base)
             ok, check = T.variance_gate(x, gate)
-            net.forward(x.view(1, H, W, 8), base.view(1, H, W, 3))  # warm-up
+            net.forward(x.view(1, h, w, 8), base.view(1, h, w, 3))  # warm-up
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             for _ in range(5):
-                pred = net.forward(x.view(1, H, W, 8), base.view(1, H, W, 3))
+                pred = net.forward(x.view(1, h, w, 8), base.view(1, h, w, 3))
             b.record(stream)
             torch.cuda.synchronize()
             dn_ms = a.elapsed_time(b) / 5
             ps_dn, me_dn = T.psnr(pred.reshape(P, 3), ref)
-            prog = T.progressive(r, cam, p, 6_000_000, [4, 8, 16, 32, 64, 128])
+            prog = T.progressive(r, cam, p, 6_000_000, list(counts))
             curve = {n: T.psnr(T.mean_rgb(v), ref)[0] for n, v in prog.items()}
             s2 = T.noise_model(curve, ref_ens)
             n_same = T.n_model(s2, ref_ens, ps_dn)
@@ -408,6 +411,68 @@ def run_trajectory(args, rank, world):
                                    f"(distance 7) x {E} ensembles, one captured CUDA graph per method",
                        "gaussians": n, "resolution": [Wt, Ht], "cameras": ncam, "ensembles_per_camera": E},
             "methods": rows}
+    print(json.dumps(line))
+    r.close()
+    return 0
+
+
+def run_stress(args, rank, world):
+    """Configuration 5 (one line, not the default): the cluster generator scaled to 6,000,000
+    Gaussians (SH3), PBVR Extinction C3+R with a per-splat cap of 65,536 at 3840x2160, near / mid /
+    far orbit views. Per view: ms per ensemble of the plain path (CUDA events over 4 ensembles),
+    the algorithmic GB/s of each stage, and the denoised 4-ensemble frame against the plain 64-
+    and 256-ensemble accumulations (PSNR and max abs error against a reference of --stress-ref
+    ensembles with disjoint seeds, ms per frame)."""
+    import torch
+    pkg = load_package()
+    from gps_pbvr_web_b200 import scenes
+    n = args.stress_gaussians
+    sw, sh_ = (int(v) for v in args.stress_res.lower().split("x"))
+    splats, sh, deg = pkg.load_ply(scenes.cluster_scene(n, seed=0, degree=3))
+    stream = torch.cuda.Stream()
+    r = pkg.GpsRenderer(sw, sh_, 1)
+    r.set_stream(stream.cuda_stream)
+    r.set_gaussians_sh(splats, sh, deg)
+    p = pkg.RenderParams(spp_side=1, max_points_per_splat=args.stress_cap, method=pkg.Method.Extinction)
+    p.pbvr.calibration = pkg.Calibration.PerSplatFootprint
+    p.pbvr.radial_correction = True
+    cams = [(name, pkg.OrbitCamera(target=(0.0, 0.0, 0.0), distance=d, yaw=0.6, pitch=0.25, up=(0.0, -1.0, 0.0),
+                                   fov_y=0.9).to_camera(sw, sh_)) for name, d in VIEWS]
+    per_view, stages = {}, {}
+    P = sw * sh_
+    for name, cam in cams:
+        r.reset_accum()
+        r.render_ensembles(cam, p, 1, 1)  # warm-up
+        r.reset_stats()
+        r.profile_enable(True)
+        p0 = r.profile()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r.reset_accum()
+        a.record(stream)
+        r.render_ensembles(cam, p, 1, 4)
+        b.record(stream)
+        torch.cuda.synchronize()
+        per_view[name] = a.elapsed_time(b) / 4
+        prof, st = r.profile(), r.read_stats()
+        rows = {}
+        for sname in ["particles", "count_scan", "resolve", "clear", "geometry"]:
+            launches = prof["launches"][sname] - p0["launches"][sname]
+            ms = prof["ms"][sname] - p0["ms"][sname]
+            if launches and ms > 0:
+                byts = algorithmic_bytes_per_launch(sname, st.subpixel_writes / launches, st.list_entries / launches,
+                                                    4, n, P)
+                rows[sname] = {"ms": ms, "launches": launches, "alg_GBps": byts * launches / (ms / 1e3) / 1e9}
+        stages[name] = {"stages": rows, "particles": st.particles, "points": st.points,
+                        "subpixel_writes": st.subpixel_writes}
+    dnz = denoise_measure(pkg, r, stream, cams, p, per_view, ref_ens=args.stress_ref, w=sw, h=sh_,
+                          counts=(4, 16, 64, 256) if args.stress_ref > 256 else (4, 16, 64))
+    line = {"metric": "stress: denoised 4-ensemble frames vs plain 64 / 256 ensembles", "unit": "dB, ms",
+            "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": f"{n} synthetic Gaussians SH3, {sw}x{sh_} spp1, cap {args.stress_cap}, "
+                                   "PBVR Extinction C3+R, near/mid/far orbit (2.5/7/20)",
+                       "gaussians": n, "resolution": [sw, sh_], "cap": args.stress_cap,
+                       "reference_ensembles": args.stress_ref},
+            "ms_per_ensemble": per_view, "per_view": stages, "denoise": dnz}
     print(json.dumps(line))
     r.close()
     return 0
@@ -594,9 +659,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-micro", action="store_true", help="skip the scan/sort HBM measurements")
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoised-vs-plain PSNR measurement")
-    ap.add_argument("--config", default="default", choices=["default", "trajectory"],
-                    help="trajectory: the 2M-Gaussian 1080p 16-camera orbit through one captured graph")
+    ap.add_argument("--config", default="default", choices=["default", "trajectory", "stress"],
+                    help="trajectory: the 2M-Gaussian 1080p 16-camera orbit through one captured graph; "
+                         "stress: the 6M-Gaussian 3840x2160 scene with the denoiser in the loop")
     ap.add_argument("--traj-gaussians", type=int, default=2_000_000)
+    ap.add_argument("--stress-gaussians", type=int, default=6_000_000)
+    ap.add_argument("--stress-res", default="3840x2160")
+    ap.add_argument("--stress-cap", type=int, default=65536)
+    ap.add_argument("--stress-ref", type=int, default=256, help="ensembles of the stress reference")
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64)
     ap.add_argument("--views", default="near,mid,far", help="subset of the views (small profiling cases)")
     ap.add_argument("--ensembles", type=int, default=ENS, help="ensembles per view (small profiling cases)")
@@ -608,6 +678,8 @@ def main():
         return run_reference(args, rank, world)
     if args.config == "trajectory":
         return run_trajectory(args, rank, world)
+    if args.config == "stress":
+        return run_stress(args, rank, world)
     return run_b200(args, rank, world)
 
 
