@@ -32,6 +32,8 @@ def _params(method, cal, radial=True, jitter=True, centre=False):
 CASES = [
     ("Extinction C3+R", PKG.Method.Extinction, PKG.Calibration.PerSplatFootprint, True, True),
     ("Extinction C3 no-jitter", PKG.Method.Extinction, PKG.Calibration.PerSplatFootprint, False, False),
+    ("Extinction C1+R", PKG.Method.Extinction, PKG.Calibration.ObjectZoom, True, True),
+    ("Proportional C2+R", PKG.Method.Proportional, PKG.Calibration.PerSplatDepth, True, True),
     ("ViewConditioned C0 +R", PKG.Method.ViewConditioned, PKG.Calibration.None_, True, True),
 ]
 
