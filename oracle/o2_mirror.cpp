@@ -1024,7 +1024,8 @@ int o2_fast_check(const gpsb_gaussian* g, uint32_t n, const float* sh, uint32_t 
 void o2_fmath_eval(int which, const float* in, float* out, size_t n) {
     for (size_t i = 0; i < n; ++i) {
         float x = in[i];
-        out[i] = which == 0 ? gx::exp(x) : which == 1 ? gx::log(x) : which == 2 ? gx::sin(x) : which == 3 ? gx::cos(x) : gx::pow(x, gxc::kInv2p4);
+        out[i] = which == 0 ? gx::exp(x) : which == 1 ? gx::log(x) : which == 2 ? gx::sin(x) : which == 3 ? gx::cos(x)
+                 : which == 5 ? gx::log_t_pos(x, gx::tab_log()) : gx::pow(x, gxc::kInv2p4);
     }
 }
 
