@@ -254,7 +254,7 @@ def o2_composite(accum, w, h, exposure, gamma_on, out_w, out_h):
 
 
 def o2_fmath(which, x):
-    """which: 0 exp, 1 log, 2 sin, 3 cos, 4 pow(x, 1/2.4)."""
+    """which: 0 exp, 1 log, 2 sin, 3 cos, 4 pow(x, 1/2.4), 5 log for positive normal arguments."""
     x = np.ascontiguousarray(x, np.float32)
     out = np.zeros_like(x)
     lib().o2_fmath_eval(which, _p(x), _p(out), x.size)
