@@ -47,6 +47,7 @@ def _declare(L):
         ("o1_psnr", D, [P, P, SZ]), ("o1_ssim", D, [P, P, SZ, SZ]),
         ("o1_look_at", None, [P, P, P, D, U32, U32, P]), ("o1_orbit_eye", None, [P, D, D, D, P, P]),
         ("o2_render_ensembles", C.c_int, [P, U32, P, U32, P, U32, U32, U32, P, P, U32, U32, P, P, P, P]),
+        ("o2_render_ensembles_mt", C.c_int, [P, U32, P, U32, P, U32, U32, U32, P, P, U32, U32, P, P, P, P, U32]),
         ("o2_render_sorted", C.c_int, [P, U32, P, U32, P, U32, U32, U32, P, P, P, P, P, P]),
         ("o2_composite", C.c_int, [P, U32, U32, C.c_float, U32, U32, U32, P]),
         ("o2_fmath_eval", None, [C.c_int, P, P, SZ]),
@@ -198,8 +199,10 @@ def _o2_scene(splats, sh):
 
 
 def o2_render_ensembles(splats, sh, sh_degree, lut, w, h, spp_side, cam17, params, first_seed, count, accum=None,
-                        stats=None, want_counts=False, want_packed=False):
-    """Returns (accum (h*w,4) f32, stats (12,) u64, counts (count,n) u32 | None, packed (count,h*w*S) u64 | None)."""
+                        stats=None, want_counts=False, want_packed=False, threads=1):
+    """Returns (accum (h*w,4) f32, stats (12,) u64, counts (count,n) u32 | None, packed (count,h*w*S) u64 | None).
+    threads > 1 splits every stage over host threads (winners by a packed 64-bit minimum); the
+    results equal the sequential form's."""
     import ctypes
     g, s = _o2_scene(splats, sh)
     n = g.shape[0]
@@ -210,9 +213,9 @@ def o2_render_ensembles(splats, sh, sh_degree, lut, w, h, spp_side, cam17, param
     counts = np.zeros((count, n), np.uint32) if want_counts else None
     packed = np.zeros((count, h * w * S), np.uint64) if want_packed else None
     lut = np.ascontiguousarray(lut, np.float32)
-    lib().o2_render_ensembles(_p(g), n, _p(s), sh_degree, _p(lut), w, h, side, _p(_f64(cam17, 17)),
-                              ctypes.cast(ctypes.pointer(params), C.c_void_p), first_seed, count, _p(acc), _p(st),
-                              _p(counts), _p(packed))
+    lib().o2_render_ensembles_mt(_p(g), n, _p(s), sh_degree, _p(lut), w, h, side, _p(_f64(cam17, 17)),
+                                 ctypes.cast(ctypes.pointer(params), C.c_void_p), first_seed, count, _p(acc), _p(st),
+                                 _p(counts), _p(packed), max(1, int(threads)))
     return acc, st, counts, packed
 
 

@@ -27,6 +27,8 @@
 #include <vector>
 #include <algorithm>
 #include <cmath>
+#include <atomic>
+#include <thread>
 
 #include "../include/gpsb200.h"
 #include "../gps-pbvr-web_b200/csrc/fmath.h"
@@ -280,13 +282,23 @@ static V3 splat_colour(const Frame& f, const Scene& s, uint32_t id) {
 // ----------------------------------------------------------------------- renderer state
 struct Write { uint32_t idx, key, id; };
 
+// (key << 32) | id of a subpixel written by one of several threads: the minimum packed word is the
+// minimum depth key and, among equal keys, the minimum splat id, the same winner as the two passes
+// over the recorded writes (the single-threaded form below).
+static inline void packed_min(std::atomic<uint64_t>& w, uint64_t v) {
+    uint64_t cur = w.load(std::memory_order_relaxed);
+    while (v < cur && !w.compare_exchange_weak(cur, v, std::memory_order_relaxed)) {
+    }
+}
+
 struct Pipeline {
     const Scene& s;
     Frame f;
     uint32_t W, H, side, S;
-    std::vector<V4> proj;            // 6 x vec4 per splat
-    std::vector<uint32_t> offsets;
+    V4* proj = nullptr;              // 6 x vec4 per splat (storage owned by the caller)
     std::vector<Write> writes;       // particle writes of the depth pass, replayed by the colour pass
+    std::atomic<uint64_t>* packed = nullptr;  // threaded form: writes go straight to the packed words
+    uint64_t nwrites = 0;            // writes of the threaded form
     Stats& st;
     uint64_t running;                // stats[8] as an exact 64-bit running total
     bool overflow;                   // stats[9]
@@ -302,9 +314,15 @@ struct Pipeline {
         float det = pr.a * pr.c - pr.b * pr.b;
         return f.prm.x * (float)S * (float)2.0 * gxc::kPi * gx::sqrt_(det) * dilog(o);
     }
-    void write(uint32_t idx, float depth_z, uint32_t id) {
-        writes.push_back({idx, gx::f2b(depth_z) | 0x80000000u, id});
+    void write_key(uint32_t idx, uint32_t key, uint32_t id) {
+        if (packed) {
+            packed_min(packed[idx], ((uint64_t)key << 32) | id);
+            ++nwrites;
+        } else {
+            writes.push_back({idx, key, id});
+        }
     }
+    void write(uint32_t idx, float depth_z, uint32_t id) { write_key(idx, gx::f2b(depth_z) | 0x80000000u, id); }
 
     // emit_particle (gps_splat.wgsl:259-282)
     void emit_gps(uint32_t gid, Rng& rng, float mx, float my, float depth_z, float o, float l00, float l10, float l11) {
@@ -542,7 +560,7 @@ struct Pipeline {
             if (rng.next() >= coverage) return;
             uint32_t idx = (yy * W + xx) * samples + sub;
             st.c[0] += 1;
-            writes.push_back({idx, gx::f2b(a.z) | 0x80000000u, i});
+            write_key(idx, gx::f2b(a.z) | 0x80000000u, i);
         } else if (f.pbvr[0] == 0u) {
             emit_gps(i, rng, a.x, a.y, a.z, a.w, b.x, b.y, b.z);
         } else {
@@ -750,16 +768,40 @@ static Scene make_scene(const gpsb_gaussian* g, uint32_t n, const float* sh, uin
     return s;
 }
 
+// Runs fn(begin, end, thread) over [0, n) in chunks taken by `threads` threads in turn.
+template <class F>
+static void parallel_chunks(uint32_t n, unsigned threads, uint32_t chunk, F fn) {
+    if (threads <= 1u) {
+        fn(0u, n, 0u);
+        return;
+    }
+    std::atomic<uint64_t> next{0};
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < threads; ++t)
+        pool.emplace_back([&, t] {
+            for (;;) {
+                const uint64_t b = next.fetch_add(chunk);
+                if (b >= n) break;
+                fn((uint32_t)b, (uint32_t)std::min<uint64_t>(n, b + chunk), t);
+            }
+        });
+    for (auto& th : pool) th.join();
+}
+
 extern "C" {
 
 // render_ensembles (gps.rs:861-925) for `count` ensembles, in the reference's order.
 // accum: W*H*4 floats (in/out). stats: 16 u64 (in/out) in gpsb_stats field order.
 // counts_out (nullable): count*n u32 per-splat counts after the cap (0 for the primitive path).
 // packed_out (nullable): count*W*H*S u64 packed (depth key << 32 | winner id).
-int o2_render_ensembles(const gpsb_gaussian* g, uint32_t n, const float* sh, uint32_t sh_degree,
-                        const float* lut, uint32_t W, uint32_t H, uint32_t side,
-                        const gpsb_camera* cam, const gpsb_params* prm, uint32_t first_seed, uint32_t count,
-                        float* accum, uint64_t* stats, uint32_t* counts_out, uint64_t* packed_out) {
+// threads <= 1: the literal sequential form (two passes over the recorded writes). threads > 1:
+// every stage split over splats (prepare, particles) or pixels (resolve), each subpixel's winner
+// taken by a packed 64-bit minimum; results are identical to the sequential form (tested).
+int o2_render_ensembles_mt(const gpsb_gaussian* g, uint32_t n, const float* sh, uint32_t sh_degree,
+                           const float* lut, uint32_t W, uint32_t H, uint32_t side,
+                           const gpsb_camera* cam, const gpsb_params* prm, uint32_t first_seed, uint32_t count,
+                           float* accum, uint64_t* stats, uint32_t* counts_out, uint64_t* packed_out,
+                           uint32_t threads) {
     side = std::max(1u, std::min(side, 4u));
     Scene s = make_scene(g, n, sh, sh_degree, lut);
     Stats st;
@@ -769,70 +811,133 @@ int o2_render_ensembles(const gpsb_gaussian* g, uint32_t n, const float* sh, uin
     for (int k = 0; k < 12; ++k) st.c[k] = stats[k];
     const uint32_t S = side * side;
     const size_t nsub = (size_t)W * H * S;
-    std::vector<uint32_t> depth(nsub), winner(nsub);
+    const unsigned T = std::max(1u, threads);
+    const bool mt = T > 1u;
+    std::vector<uint32_t> depth(mt ? 0 : nsub), winner(mt ? 0 : nsub);
+    std::vector<std::atomic<uint64_t>> words(mt ? nsub : 0);
+    std::vector<V4> proj((size_t)n * 6u);
+    std::vector<uint32_t> offsets(n);
+    std::vector<Stats> ts(T);
     bool use_particles = (prm->path == GPSB_PATH_PARTICLE || prm->method != GPSB_METHOD_GPS) && n > 0;
     for (uint32_t e = 0; e < count; ++e) {
-        Pipeline pl(s, st);
-        pl.f = make_frame(s, *cam, *prm, W, H, side, first_seed + e);
-        pl.W = W; pl.H = H; pl.side = side; pl.S = S;
-        pl.proj.assign((size_t)n * 6u, V4{0, 0, 0, 0});
-        pl.running = 0;
-        pl.overflow = false;
+        const Frame fr = make_frame(s, *cam, *prm, W, H, side, first_seed + e);
+        for (auto& t : ts) memset(&t, 0, sizeof t);
+        std::vector<uint64_t> nwrites(T, 0);
+        auto pipeline = [&](unsigned t) {
+            Pipeline pl(s, mt ? ts[t] : st);
+            pl.f = fr;
+            pl.W = W; pl.H = H; pl.side = side; pl.S = S;
+            pl.proj = proj.data();
+            pl.running = 0;
+            pl.overflow = false;
+            if (mt) pl.packed = words.data();
+            return pl;
+        };
+        std::fill(proj.begin(), proj.end(), V4{0, 0, 0, 0});
         // clear_buffers (gps_splat.wgsl:336-347)
-        std::fill(depth.begin(), depth.end(), gxc::kEmpty);
-        std::fill(winner.begin(), winner.end(), gxc::kEmpty);
+        if (mt) {
+            for (auto& w : words) w.store(~0ull, std::memory_order_relaxed);
+        } else {
+            std::fill(depth.begin(), depth.end(), gxc::kEmpty);
+            std::fill(winner.begin(), winner.end(), gxc::kEmpty);
+        }
         st.c[8] += 1;
+        bool overflow = false;
+        std::vector<Write> seq_writes;
         if (use_particles) {
-            pl.offsets.assign(n, 0u);
-            for (uint32_t i = 0; i < n; ++i) pl.offsets[i] = pl.prepare(i);
-            if (counts_out) memcpy(counts_out + (size_t)e * n, pl.offsets.data(), (size_t)n * 4);
-            for (uint32_t i = 0; i < n; ++i) st.c[11] += pl.offsets[i] ? 1u : 0u;
+            parallel_chunks(n, T, 4096u, [&](uint32_t b, uint32_t en, unsigned t) {
+                Pipeline pl = pipeline(t);
+                for (uint32_t i = b; i < en; ++i) offsets[i] = pl.prepare(i);
+            });
+            if (counts_out) memcpy(counts_out + (size_t)e * n, offsets.data(), (size_t)n * 4);
+            uint64_t total = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                st.c[11] += offsets[i] ? 1u : 0u;
+                total += offsets[i];
+            }
+            // prepare's exact u32 overflow detection of the running total (gps_splat.wgsl:635-639) and
             // finalize_dispatch (gps_splat.wgsl:648-663): skip the ensemble on u32 overflow
-            if (pl.overflow) {
+            overflow = total > 0xFFFFFFFFull;
+            if (overflow) {
                 st.c[7] += 1;
             } else {
-                for (uint32_t i = 0; i < n; ++i)
-                    for (uint32_t k = 0; k < pl.offsets[i]; ++k) pl.particle(i, k);
+                parallel_chunks(n, T, 16u, [&](uint32_t b, uint32_t en, unsigned t) {
+                    Pipeline pl = pipeline(t);
+                    for (uint32_t i = b; i < en; ++i)
+                        for (uint32_t k = 0; k < offsets[i]; ++k) pl.particle(i, k);
+                    nwrites[t] += pl.nwrites;
+                    if (!mt) seq_writes.swap(pl.writes);
+                });
             }
         } else {
             if (counts_out) memset(counts_out + (size_t)e * n, 0, (size_t)n * 4);
-            for (uint32_t i = 0; i < n; ++i) pl.splat_pass(i);
+            parallel_chunks(n, T, 16u, [&](uint32_t b, uint32_t en, unsigned t) {
+                Pipeline pl = pipeline(t);
+                for (uint32_t i = b; i < en; ++i) pl.splat_pass(i);
+                nwrites[t] += pl.nwrites;
+                if (!mt) seq_writes.swap(pl.writes);
+            });
         }
-        st.c[10] += pl.writes.size();
-        // depth pass, then colour pass among the depth winners (gps_splat.wgsl:276-281)
-        for (const Write& w : pl.writes) depth[w.idx] = std::min(depth[w.idx], w.key);
-        for (const Write& w : pl.writes)
-            if (depth[w.idx] == w.key) winner[w.idx] = std::min(winner[w.idx], w.id);
+        if (mt) {
+            for (unsigned t = 0; t < T; ++t) {
+                for (int k = 0; k < 16; ++k) st.c[k] += ts[t].c[k];
+                st.c[10] += nwrites[t];
+                memset(&ts[t], 0, sizeof ts[t]);
+            }
+        } else {
+            st.c[10] += seq_writes.size();
+            // depth pass, then colour pass among the depth winners (gps_splat.wgsl:276-281)
+            for (const Write& w : seq_writes) depth[w.idx] = std::min(depth[w.idx], w.key);
+            for (const Write& w : seq_writes)
+                if (depth[w.idx] == w.key) winner[w.idx] = std::min(winner[w.idx], w.id);
+        }
+        auto word = [&](size_t j) -> uint64_t {
+            return mt ? words[j].load(std::memory_order_relaxed) : ((uint64_t)depth[j] << 32) | winner[j];
+        };
         if (packed_out) {
             uint64_t* out = packed_out + (size_t)e * nsub;
-            for (size_t j = 0; j < nsub; ++j) out[j] = ((uint64_t)depth[j] << 32) | winner[j];
+            for (size_t j = 0; j < nsub; ++j) out[j] = word(j);
         }
         // resolve (gps_splat.wgsl:362-386)
-        if (!pl.overflow) {
-            for (uint32_t pix = 0; pix < W * H; ++pix) {
-                V3 sum = {(float)0.0, (float)0.0, (float)0.0};
-                for (uint32_t k = 0; k < S; ++k) {
-                    size_t j = (size_t)pix * S + k;
-                    if (depth[j] == gxc::kEmpty) {
-                        sum = {sum.x + pl.f.bg.x, sum.y + pl.f.bg.y, sum.z + pl.f.bg.z};
-                    } else if (winner[j] == gxc::kEmpty) {
-                        st.c[4] += 1;
-                        sum = {sum.x + pl.f.bg.x, sum.y + pl.f.bg.y, sum.z + pl.f.bg.z};
-                    } else {
-                        V3 c = splat_colour(pl.f, s, winner[j]);
-                        sum = {sum.x + c.x, sum.y + c.y, sum.z + c.z};
+        if (!overflow) {
+            parallel_chunks(W * H, T, 4096u, [&](uint32_t b, uint32_t en, unsigned t) {
+                Stats& sx = mt ? ts[t] : st;
+                for (uint32_t pix = b; pix < en; ++pix) {
+                    V3 sum = {(float)0.0, (float)0.0, (float)0.0};
+                    for (uint32_t k = 0; k < S; ++k) {
+                        const uint64_t w = word((size_t)pix * S + k);
+                        const uint32_t dk = (uint32_t)(w >> 32), win = (uint32_t)w;
+                        if (dk == gxc::kEmpty) {
+                            sum = {sum.x + fr.bg.x, sum.y + fr.bg.y, sum.z + fr.bg.z};
+                        } else if (win == gxc::kEmpty) {
+                            sx.c[4] += 1;
+                            sum = {sum.x + fr.bg.x, sum.y + fr.bg.y, sum.z + fr.bg.z};
+                        } else {
+                            V3 c = splat_colour(fr, s, win);
+                            sum = {sum.x + c.x, sum.y + c.y, sum.z + c.z};
+                        }
                     }
+                    float* a = accum + (size_t)pix * 4u;
+                    a[0] = a[0] + gx::div_(sum.x, (float)S);
+                    a[1] = a[1] + gx::div_(sum.y, (float)S);
+                    a[2] = a[2] + gx::div_(sum.z, (float)S);
+                    a[3] = a[3] + (float)1.0;
                 }
-                float* a = accum + (size_t)pix * 4u;
-                a[0] = a[0] + gx::div_(sum.x, (float)S);
-                a[1] = a[1] + gx::div_(sum.y, (float)S);
-                a[2] = a[2] + gx::div_(sum.z, (float)S);
-                a[3] = a[3] + (float)1.0;
-            }
+            });
+            if (mt)
+                for (unsigned t = 0; t < T; ++t) st.c[4] += ts[t].c[4];
         }
     }
     for (int k = 0; k < 12; ++k) stats[k] = st.c[k];
     return 0;
+}
+
+int o2_render_ensembles(const gpsb_gaussian* g, uint32_t n, const float* sh, uint32_t sh_degree,
+                        const float* lut, uint32_t W, uint32_t H, uint32_t side,
+                        const gpsb_camera* cam, const gpsb_params* prm, uint32_t first_seed, uint32_t count,
+                        float* accum, uint64_t* stats, uint32_t* counts_out, uint64_t* packed_out) {
+    return o2_render_ensembles_mt(g, n, sh, sh_degree, lut, W, H, side, cam, prm, first_seed, count, accum, stats,
+                                  counts_out, packed_out, 1u);
 }
 
 // sp_project + stable radix order + front-to-back f32 blend (the sorted path; see the file
@@ -987,7 +1092,8 @@ int o2_fast_check(const gpsb_gaussian* g, uint32_t n, const float* sh, uint32_t 
         Pipeline pl(s, st);
         pl.f = make_frame(s, *cam, *prm, W, H, side, first_seed + e);
         pl.W = W; pl.H = H; pl.side = side; pl.S = side * side;
-        pl.proj.assign((size_t)n * 6u, V4{0, 0, 0, 0});
+        std::vector<V4> proj((size_t)n * 6u, V4{0, 0, 0, 0});
+        pl.proj = proj.data();
         pl.running = 0;
         pl.overflow = false;
         std::vector<uint32_t> cnt(n);
