@@ -7,8 +7,9 @@ of include/gpsb200.h. `gps` mirrors the reference's Rust renderer API in Python.
 """
 from . import abi
 from .gps import (Calibration, GpsError, GpsRenderer, GpuStats, Method, OracleCamera, OrbitCamera, PbvrParams,
-                  RenderParams, RenderPath, default_params, estimate_memory, load_ply, load_ply_device, radius_lut)
+                  RenderParams, RenderPath, debug_fmath, default_params, estimate_memory, load_ply, load_ply_device,
+                  radius_lut)
 
 __all__ = ["abi", "Calibration", "GpsError", "GpsRenderer", "GpuStats", "Method", "OracleCamera", "OrbitCamera",
-           "PbvrParams", "RenderParams", "RenderPath", "default_params", "estimate_memory", "load_ply", "load_ply_device",
+           "PbvrParams", "RenderParams", "RenderPath", "debug_fmath", "default_params", "estimate_memory", "load_ply", "load_ply_device",
            "radius_lut"]

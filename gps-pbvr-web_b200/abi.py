@@ -84,6 +84,7 @@ P = C.c_void_p
 U32 = C.c_uint32
 SZ = C.c_size_t
 ST = C.c_int
+U64 = C.c_uint64
 
 # name -> (restype, argtypes); every function declared in include/gpsb200.h
 SIGNATURES = {
@@ -132,6 +133,8 @@ SIGNATURES = {
     "gpsb_debug_read_counts": (ST, [P, U32, P]),
     "gpsb_debug_read_subpixels": (ST, [P, U32, P]),
     "gpsb_debug_error_word": (U32, [P]),
+    "gpsb_debug_particle_seeds": (ST, [P, U32, U64, U32, P]),
+    "gpsb_debug_fmath": (ST, [U32, P, P, U64]),
     "gpsb_load_ply": (ST, [P, SZ, P, P, P, P]),
     "gpsb_load_ply_device": (ST, [P, SZ, P, P, P, P, P]),
     "gpsb_ply_last_error": (C.c_char_p, []),

@@ -96,6 +96,9 @@ void launch_features(const FrameConst& fc, const unsigned long long* sub, const 
 void launch_resolve(const FrameConst& fc, const unsigned long long* sub, const EnsTotal* etot, const float4* colour,
                     uint32_t E, float4* accum, unsigned long long* stats, cudaStream_t st);
 void launch_add_stat(unsigned long long* stats, int word, unsigned long long v, cudaStream_t st);
+void launch_debug_fmath(uint32_t which, const float* in, float* out, uint64_t n, cudaStream_t st);
+void launch_debug_seeds(const uint2* list, uint32_t nonzero, uint64_t p0, uint32_t n, uint32_t seed, uint32_t* out,
+                        cudaStream_t st);
 
 // sorted path (sorted.cu)
 struct SortedBuffers;

@@ -1237,6 +1237,71 @@ void launch_add_stat(unsigned long long* stats, int word, unsigned long long v, 
     k_add_stat<<<1, 1, 0, st>>>(stats, word, v);
 }
 
+// ----------------------------------------------------------------------------- debug probes
+// The shared maths evaluated on the device, as the kernels evaluate it: which 0 exp, 1 log, 2 sin,
+// 3 cos, 4 log for positive normal arguments, with the tables staged in shared memory (the
+// particle kernel's form); which | 8: the same functions reading the global tables (the form of
+// the other kernels).
+__global__ void __launch_bounds__(256) k_debug_fmath(uint32_t which, const float* __restrict__ in,
+                                                     float* __restrict__ out, uint64_t n) {
+    __shared__ __align__(16) float s_tab[kTabFloats];
+    const FTabs T = stage_tabs(s_tab);
+    __syncthreads();
+    const bool global = (which & 8u) != 0u;
+    const uint32_t op = which & 7u;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float x = in[i];
+        float y, sn, cs;
+        if (op == 0u) {
+            y = global ? gx::exp(x) : gx::exp_t(x, T.ex);
+        } else if (op == 1u) {
+            y = global ? gx::log(x) : gx::log_t(x, T.lg);
+        } else if (op == 4u) {
+            y = gx::log_t_pos(x, global ? gx::tab_log() : T.lg);
+        } else {
+            if (global) gx::sincos(x, &sn, &cs); else gx::sincos_t(x, T.sc, &sn, &cs);
+            y = op == 2u ? sn : cs;
+        }
+        out[i] = y;
+    }
+}
+
+void launch_debug_fmath(uint32_t which, const float* in, float* out, uint64_t n, cudaStream_t st) {
+    if (n == 0) return;
+    const uint64_t blocks = (n + 255) / 256;
+    k_debug_fmath<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(which, in, out, n);
+}
+
+// For each particle p in [p0, p0 + n) of one ensemble's compact (splat id, offset) list: its splat
+// i (the last entry with offset <= p, found with the particle kernel's 32-ary warp search), its
+// index k within the splat and its stream seed particle_seed(i, k + 1, seed). out: 3 words per
+// particle. One warp per 32 consecutive particles; the host checks p0 + n <= the list's total.
+__global__ void __launch_bounds__(128) k_debug_seeds(const uint2* __restrict__ L, uint32_t nonzero, uint64_t p0,
+                                                     uint32_t n, uint32_t seed, uint32_t* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
+    if (base >= n) return;  // warp-uniform
+    const uint32_t m = n - base < 32u ? n - base : 32u;
+    for (uint32_t q = 0; q < m; ++q) {
+        const uint64_t p = p0 + base + q;
+        const uint32_t j = warp_last_le(L, 0u, nonzero, p, lane);
+        if (lane == 0) {
+            const uint2 e = L[j];
+            const uint32_t k = (uint32_t)(p - e.y);
+            out[3u * (base + q)] = e.x;
+            out[3u * (base + q) + 1u] = k;
+            out[3u * (base + q) + 2u] = gx::particle_seed(e.x, k + 1u, seed);
+        }
+    }
+}
+
+void launch_debug_seeds(const uint2* list, uint32_t nonzero, uint64_t p0, uint32_t n, uint32_t seed, uint32_t* out,
+                        cudaStream_t st) {
+    if (n == 0 || nonzero == 0) return;
+    const uint32_t warps = (n + 31u) / 32u;
+    k_debug_seeds<<<(warps + 3u) / 4u, 128, 0, st>>>(list, nonzero, p0, n, seed, out);
+}
+
 int device_sm_count(int device) {
     int n = 0;
     cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);

@@ -74,6 +74,7 @@ struct gpsb_renderer {
     DevBuf sub, clist, lookback, etot, counters;
     uint32_t batch_cap = 0;
     uint32_t last_batch = 0;     // ensembles in the last batch rendered
+    uint32_t last_seed = 0;      // seed of its first ensemble
     bool last_particle = false;  // whether it used the particle path
     // sorted path
     SortedState sorted;
@@ -324,6 +325,7 @@ static gpsb_status render_batch(gpsb_renderer* r, const FrameConst& f, bool part
         }
     }
     r->last_batch = E;
+    r->last_seed = first_seed;
     r->last_particle = particles;
     return GPSB_OK;
 }
@@ -929,6 +931,37 @@ gpsb_status gpsb_debug_read_counts(gpsb_renderer* r, uint32_t slot, uint32_t* co
         uint32_t end = j + 1 < t.nonzero ? L[j + 1].y : (uint32_t)t.particles;
         if (L[j].x < r->n) counts[L[j].x] = end - L[j].y;
     }
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_debug_particle_seeds(gpsb_renderer* r, uint32_t slot, uint64_t first_particle, uint32_t n,
+                                      uint32_t* out) {
+    if (!r || (n && !out)) return fail(r, GPSB_ERR_INVALID_ARGUMENT, "null argument");
+    if (!r->last_particle || slot >= r->last_batch) return fail(r, GPSB_ERR_STATE, "slot not in the last particle-path batch");
+    cudaSetDevice(r->device);
+    EnsTotal t;
+    CK(r, cudaMemcpyAsync(&t, r->etot.as<EnsTotal>() + slot, sizeof t, cudaMemcpyDeviceToHost, r->stream), "read totals");
+    CK(r, cudaStreamSynchronize(r->stream), "synchronise");
+    if (t.flags != 0u) return fail(r, GPSB_ERR_STATE, "the ensemble was skipped");
+    if (first_particle > t.particles || n > t.particles - first_particle)
+        return fail(r, GPSB_ERR_INVALID_ARGUMENT, "particle range beyond the ensemble's total");
+    if (n == 0) return GPSB_OK;
+    CK(r, r->dbg.ensure((size_t)n * 12), "debug buffer");
+    launch_debug_seeds(r->clist.as<uint2>() + (size_t)slot * r->n, t.nonzero, first_particle, n, r->last_seed + slot,
+                       r->dbg.as<uint32_t>(), r->stream);
+    CK(r, cudaGetLastError(), "seed probe kernel");
+    CK(r, cudaMemcpyAsync(out, r->dbg.p, (size_t)n * 12, cudaMemcpyDeviceToHost, r->stream), "read seeds");
+    CK(r, cudaStreamSynchronize(r->stream), "synchronise");
+    return GPSB_OK;
+}
+
+gpsb_status gpsb_debug_fmath(uint32_t which, const float* in_dev, float* out_dev, uint64_t n) {
+    if ((which & 7u) > 4u || (which & ~15u) != 0u) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "which: 0..4, | 8");
+    if (n && (!in_dev || !out_dev)) return fail(nullptr, GPSB_ERR_INVALID_ARGUMENT, "null buffer");
+    launch_debug_fmath(which, in_dev, out_dev, n, nullptr);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);
+    if (e != cudaSuccess) return fail(nullptr, GPSB_ERR_CUDA, std::string("fmath probe: ") + cudaGetErrorString(e));
     return GPSB_OK;
 }
 

@@ -247,6 +247,14 @@ def load_ply_device(data: bytes):
     return g, sh[: n.value * 3 * per], d.value
 
 
+def debug_fmath(which: int, x_dev, out_dev):
+    """The shared exp (0) / log (1) / sin (2) / cos (3) / positive-normal log (4) evaluated on the
+    device as the kernels evaluate them (which | 8: global tables); x_dev/out_dev are float32 CUDA
+    tensors of the same size."""
+    _check(None, abi.lib().gpsb_debug_fmath(which, C.c_void_p(x_dev.data_ptr()), C.c_void_p(out_dev.data_ptr()),
+                                            x_dev.numel()))
+
+
 def load_ply(data: bytes):
     """gps-io load_ply + activation + GpuGaussian::from_activated: (splats (n,16) f32, sh_rest f32, degree)."""
     L = abi.lib()
@@ -436,6 +444,13 @@ class GpsRenderer:
         s = self.spp_side()
         out = np.zeros(w * h * s * s, np.uint64)
         self._ck(self._L.gpsb_debug_read_subpixels(self._r, slot, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def debug_particle_seeds(self, slot: int, first_particle: int, n: int) -> np.ndarray:
+        """(n, 3) u32: splat, index within the splat and stream seed of particles first_particle..
+        of ensemble `slot` of the last particle-path render, as the particle kernel derives them."""
+        out = np.zeros((n, 3), np.uint32)
+        self._ck(self._L.gpsb_debug_particle_seeds(self._r, slot, first_particle, n, out.ctypes.data_as(C.c_void_p)))
         return out
 
     def set_footprint(self, footprint_subpixels=1, adaptive_kappa=0.0, footprint_max=4, compensate_blur=False):

@@ -290,6 +290,18 @@ gpsb_status gpsb_debug_read_counts(gpsb_renderer* r, uint32_t slot, uint32_t* co
 gpsb_status gpsb_debug_read_subpixels(gpsb_renderer* r, uint32_t slot, uint64_t* packed);
 /* Device-side error word (bounded waits that gave up); 0 when healthy. */
 uint32_t gpsb_debug_error_word(gpsb_renderer* r);
+/* Stream seeds of particles first_particle .. first_particle + n - 1 of ensemble `slot` of the
+ * last particle-path render call, as the particle kernel derives them: out[3 j .. 3 j + 2] =
+ * (splat i, index k within the splat, particle_seed(i, k + 1, seed of the ensemble)), the splat
+ * found in the compact list by the particle kernel's search (shaders/gps_splat.wgsl:63-68,
+ * 667-680; crates/gps-core/src/lib.rs:450-465). Synchronous; host output of 3 n words. */
+gpsb_status gpsb_debug_particle_seeds(gpsb_renderer* r, uint32_t slot, uint64_t first_particle, uint32_t n,
+                                      uint32_t* out);
+/* The shared exp/log/sin/cos evaluated on the current device exactly as the kernels evaluate
+ * them: which 0 exp, 1 log, 2 sin, 3 cos, 4 log of a positive normal argument, tables in shared
+ * memory (the particle kernel's form); which | 8 reads the global tables (the other kernels'
+ * form). in_dev/out_dev: n floats of device memory. Synchronous (legacy default stream). */
+gpsb_status gpsb_debug_fmath(uint32_t which, const float* in_dev, float* out_dev, uint64_t n);
 
 /* Launch-shape tuning (no reference counterpart). Zero fields keep the current value.
  *   sort_digit_bits        radix digit width of the depth sort: 4, 6 or 8 (default 8)
