@@ -354,7 +354,7 @@ constexpr uint32_t kNoAllocMaxN = 1u << 21;
 constexpr uint32_t kNoAllocTiles = (kNoAllocMaxN + RsShape<8>::tile - 1) / RsShape<8>::tile;
 constexpr uint32_t kNoAllocPasses = 4;
 constexpr size_t kNoAllocHistWords = kNoAllocPasses * 256;
-constexpr size_t kNoAllocCounterWords = 16;  // per-pass tile counters, then the default error word
+constexpr size_t kNoAllocCounterWords = 16;  // per-pass tile counters (padded)
 constexpr size_t kNoAllocWords = kNoAllocHistWords + kNoAllocCounterWords + (size_t)kNoAllocPasses * kNoAllocTiles * 256;
 static __device__ __align__(256) uint32_t g_noalloc_sort_scratch[kNoAllocWords];
 
@@ -365,12 +365,15 @@ cudaError_t radix_sort_pairs(RadixScratch& s, uint32_t* ka, uint32_t* va, uint32
     return radix_impl<8>(s, ka, va, kb, vb, n, key_bits, err, st);
 }
 
-// Device address of g_noalloc_sort_scratch on the current device, resolved once per device. In host
-// code the array's name is only a host-side stand-in, so the address comes from
-// cudaGetSymbolAddress with the device current; it is cached per device ordinal.
-static void* noalloc_scratch_address(cudaError_t* err) {
+// Device address of g_noalloc_sort_scratch on the current device. In host code the array's name is
+// only a host-side stand-in, so the address comes from cudaGetSymbolAddress with the device
+// current. It is looked up again on every call whose stream is not capturing (so a device reset,
+// which reloads the module, never leaves a stale address behind) and kept per device ordinal for
+// calls made while `st` is being captured into a graph, which must follow one uncaptured call.
+static void* noalloc_scratch_address(cudaStream_t st, cudaError_t* err, bool* capture_without_setup) {
     static std::mutex mu;
     static void* addr[256] = {};
+    *capture_without_setup = false;
     int dev = 0;
     *err = cudaGetDevice(&dev);
     if (*err != cudaSuccess) return nullptr;
@@ -378,12 +381,17 @@ static void* noalloc_scratch_address(cudaError_t* err) {
         *err = cudaErrorInvalidDevice;
         return nullptr;
     }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    *err = cudaStreamIsCapturing(st, &cs);
+    if (*err != cudaSuccess) return nullptr;
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         *err = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
         if (*err != cudaSuccess) return nullptr;
         addr[dev] = p;
+    } else if (!addr[dev]) {
+        *capture_without_setup = true;
     }
     return addr[dev];
 }
@@ -820,25 +828,30 @@ extern "C" gpsb_status gpsb_sort_pairs_noalloc(uint32_t* keys_in, uint32_t* vals
         return GPSB_ERR_INVALID_ARGUMENT;
     }
     if (n == 0) return GPSB_OK;
-    if (!keys_in || !vals_in || !keys_out || !vals_out) {
-        snprintf(g_noalloc_error, sizeof g_noalloc_error, "gpsb_sort_pairs_noalloc: null buffer");
+    if (!keys_in || !vals_in || !keys_out || !vals_out || !err_dev) {
+        snprintf(g_noalloc_error, sizeof g_noalloc_error, "gpsb_sort_pairs_noalloc: null buffer or error word");
         set_global_error(g_noalloc_error);
         return GPSB_ERR_INVALID_ARGUMENT;
     }
     cudaStream_t st = (cudaStream_t)cuda_stream;
     cudaError_t e;
-    uint32_t* base = (uint32_t*)noalloc_scratch_address(&e);
+    bool capture_without_setup = false;
+    uint32_t* base = (uint32_t*)noalloc_scratch_address(st, &e, &capture_without_setup);
     if (!base) {
-        snprintf(g_noalloc_error, sizeof g_noalloc_error, "gpsb_sort_pairs_noalloc: scratch address: %s",
-                 cudaGetErrorString(e));
+        if (capture_without_setup)
+            snprintf(g_noalloc_error, sizeof g_noalloc_error,
+                     "gpsb_sort_pairs_noalloc: the first call on a device must come before any stream capture");
+        else
+            snprintf(g_noalloc_error, sizeof g_noalloc_error, "gpsb_sort_pairs_noalloc: scratch address: %s",
+                     cudaGetErrorString(e));
         set_global_error(g_noalloc_error);
-        return GPSB_ERR_CUDA;
+        return capture_without_setup ? GPSB_ERR_STATE : GPSB_ERR_CUDA;
     }
     const int passes = (int)((key_bits + 7) / 8);
     const uint32_t tiles = (n + RsShape<8>::tile - 1) / RsShape<8>::tile;
     uint32_t* hist = base;
     uint32_t* counters = base + kNoAllocHistWords;
-    uint32_t* err = err_dev ? err_dev : counters + kNoAllocPasses;
+    uint32_t* err = err_dev;
     uint32_t* lookback = base + kNoAllocHistWords + kNoAllocCounterWords;
     // the array keeps the previous call's contents: clear what this call needs at zero
     e = cudaMemsetAsync(base, 0, (kNoAllocHistWords + kNoAllocCounterWords) * 4, st);

@@ -352,14 +352,17 @@ gpsb_status gpsb_p0_sample(gpsb_renderer* r, uint32_t seed, uint32_t pixel_base,
  * caller; the sorted pairs are written to keys_out/vals_out and keys_in/vals_in are overwritten
  * (they are the ping-pong buffer). Its scratch is a fixed array inside this library (about
  * 1.35 MB, held by every GPU that loads the library until the process exits), which limits n to
- * 2,097,152 pairs; larger n returns GPSB_ERR_LIMIT. The first call on a device looks the array's
- * device address up (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture. Work is enqueued on cuda_stream (NULL = the legacy default stream)
- * and the call returns without waiting. Every call shares the one array, which keeps the last
- * call's contents: each call clears what it needs, but calls that overlap on the GPU (on
- * different streams, or from several threads) race and give wrong results. A bounded device-side
- * wait that gives up ORs a non-zero value into *err_dev (a device word of the caller; NULL uses a
- * word inside the array). Messages of failed calls: gpsb_last_error(NULL). */
+ * 2,097,152 pairs; larger n returns GPSB_ERR_LIMIT. Each call whose stream is not being captured
+ * looks the array's device address up (cudaGetSymbolAddress, with the call's device current), so
+ * a device reset in between is harmless; a call made while its stream is being captured uses the
+ * address of the last uncaptured call on that device, and without one it returns GPSB_ERR_STATE:
+ * make the first call on a device before any stream capture. Work is enqueued on cuda_stream
+ * (NULL = the legacy default stream) and the call returns without waiting. Every call shares the
+ * one array, which keeps the last call's contents: each call clears what it needs, but calls that
+ * overlap on the GPU (on different streams, or from several threads) race and give wrong results.
+ * err_dev is a device word of the caller and must not be NULL: a bounded device-side wait that
+ * gives up ORs a non-zero value into it (the sort's output is then not valid). Messages of failed
+ * calls: gpsb_last_error(NULL). */
 gpsb_status gpsb_sort_pairs_noalloc(uint32_t* keys_in, uint32_t* vals_in, uint32_t* keys_out,
                                     uint32_t* vals_out, uint32_t n, uint32_t key_bits,
                                     void* cuda_stream, uint32_t* err_dev);

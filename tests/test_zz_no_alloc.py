@@ -51,7 +51,7 @@ def _reference_sort(g):
     return keys, vals, key_of, np.arange(n, dtype=np.uint32)
 
 
-def _noalloc_sort(keys_in, vals_in, key_bits):
+def _noalloc_sort(keys_in, vals_in, key_bits, with_err=True):
     import torch
     L = PKG.abi.lib()
     dev = torch.device("cuda", 0)
@@ -63,7 +63,9 @@ def _noalloc_sort(keys_in, vals_in, key_bits):
     stream = torch.cuda.current_stream(dev)
     st = L.gpsb_sort_pairs_noalloc(C.c_void_p(ki.data_ptr()), C.c_void_p(vi.data_ptr()), C.c_void_p(ko.data_ptr()),
                                    C.c_void_p(vo.data_ptr()), len(keys_in), key_bits, C.c_void_p(stream.cuda_stream),
-                                   C.c_void_p(err.data_ptr()))
+                                   C.c_void_p(err.data_ptr()) if with_err else None)
+    if not with_err:
+        return st, L.gpsb_last_error(None).decode()
     assert st == 0, L.gpsb_last_error(None).decode()
     torch.cuda.synchronize(dev)
     assert int(err.item()) == 0
@@ -76,6 +78,27 @@ def test_noalloc_sort_matches_the_sorted_path_twice():
         ko, vo = _noalloc_sort(keys_in, vals_in, 24)
         assert np.array_equal(ko, keys), f"n={n}: keys differ"
         assert np.array_equal(vo, vals), f"n={n}: values differ (the sort must be stable)"
+
+
+@pytest.mark.parametrize("key_bits", [16, 32, 7])
+def test_noalloc_sort_every_pass_parity(key_bits):
+    """Two and four 8-bit passes (an even count starts from a copy of the input in the output
+    buffers) and one pass, against numpy's stable argsort, twice in a row."""
+    for n, seed in [(200_003, key_bits), (4099, key_bits + 1)]:
+        rng = np.random.default_rng(seed)
+        keys = rng.integers(0, 1 << key_bits, n, dtype=np.uint64).astype(np.uint32)
+        keys[: n // 5] = keys[n // 3]  # long runs of equal keys: stability matters
+        vals = rng.permutation(n).astype(np.uint32)
+        order = np.argsort(keys, kind="stable")
+        ko, vo = _noalloc_sort(keys, vals, key_bits)
+        assert np.array_equal(ko, keys[order]), f"key_bits={key_bits} n={n}: keys differ"
+        assert np.array_equal(vo, vals[order]), f"key_bits={key_bits} n={n}: values differ"
+
+
+def test_noalloc_sort_requires_an_error_word():
+    keys = np.arange(100, dtype=np.uint32)[::-1].copy()
+    st, msg = _noalloc_sort(keys, keys.copy(), 8, with_err=False)
+    assert st == 1 and "error word" in msg  # GPSB_ERR_INVALID_ARGUMENT
 
 
 def test_noalloc_sort_rejects_sizes_above_its_scratch():
