@@ -12,7 +12,9 @@ Multi-GPU (torchrun, one rank per GPU): every rank renders its own ensembles (se
 rank) of the same views: weak scaling, no collective on the data path; the timed region is
 bracketed by a barrier + synchronize and the max over ranks is reported.
 `--impl reference` times the reference's CPU implementation of the path (the C++ port of
-gps-core's render_particles_3d, oracle/o1_core.cpp) on the host cores, on rank 0 only.
+gps-core's render_particles_3d, oracle/o1_core.cpp) on all host cores, on rank 0 only; it reads
+the scene with the oracle's PLY reader and builds the cameras with O1's camera code, so the
+renderer library is never loaded on that arm.
 """
 import argparse
 import json
@@ -166,54 +168,112 @@ def issue_roofline(st, ms, world, clk):
 
 
 # ------------------------------------------------------------------------------ CPU reference
-def cpu_reference(pkg, splats, fraction, threads, views_cams, first_seed=1):
-    """O1 render_particles_3d (the C++ port of gps-core, with the GPU's per-splat cap) on the first
-    `fraction` of the splats (a uniform subset: the generator shuffles splats), one ensemble per
-    thread per view. Returns (ensembles/s scaled to the full scene, per-view ms/ensemble)."""
+def scenes_module():
+    """gps-pbvr-web_b200/scenes.py loaded on its own (numpy only): the reference arm builds its scene
+    without importing the renderer package."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_gpsb_scenes", os.path.join(ROOT, "gps-pbvr-web_b200", "scenes.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_inputs():
+    """The workload for the CPU arm, through the oracle alone: the seeded scene read by the oracle's
+    PLY reader (a restatement of gps-io) and the orbit cameras built by O1's camera code (a
+    restatement of gps-core's camera.rs), both equal to what the renderer receives."""
     import oracle as O
-    n = max(1, int(len(splats) * fraction))
-    g = splats[:n]
-    sc = {"pos": g[:, 0:3].astype(np.float64), "log_scale": g[:, 4:7].astype(np.float64),
-          "rot_xyzw": np.concatenate([g[:, 9:12], g[:, 8:9]], axis=1).astype(np.float64),
-          "opacity": g[:, 3].astype(np.float64), "color": g[:, 12:15].astype(np.float64)}
-    per_view = {}
-    total_s_per_ens = 0.0
-    for name, cam in views_cams:
-        t = time.perf_counter()
-        O.render_particles_3d(sc, cam.to_array(), W, H, SIDE, threads, (0.05, 0.05, 0.08), first_seed, level=3, rule=1,
-                              radial_correction=True, per_particle_seed=True, threads=threads, max_points_per_splat=CAP)
-        dt = time.perf_counter() - t
-        s_per_ens = dt / threads / (n / len(splats))  # wall seconds per full-scene ensemble at `threads` in parallel
+    from oracle import ply
+    g, _, _, _ = ply.read_ply(scenes_module().cluster_scene(N_SPLATS, seed=0, degree=3))
+    cams = []
+    for name, d in VIEWS:
+        eye = O.orbit_eye((0.0, 0.0, 0.0), d, 0.6, 0.25, (0.0, -1.0, 0.0))
+        cams.append((name, O.look_at(eye, (0.0, 0.0, 0.0), (0.0, -1.0, 0.0), 0.9, W, H)))
+    return g, cams
+
+
+def o1_call(g, cam17, seed):
+    """Wall seconds of one O1 render_particles_3d call (the C++ port of gps-core, with the GPU's
+    per-splat cap): one ensemble of the splats g on one thread."""
+    import oracle as O
+    from oracle import ply
+    sc = ply.o1_scene(g)
+    t = time.perf_counter()
+    O.render_particles_3d(sc, cam17, W, H, SIDE, 1, (0.05, 0.05, 0.08), seed, level=3, rule=1, radial_correction=True,
+                          per_particle_seed=True, threads=1, max_points_per_splat=CAP)
+    return time.perf_counter() - t
+
+
+def o1_concurrent(parts, cam17, first_seed):
+    """Runs o1_call on every splat array of `parts` at once, one host thread each (the calls release
+    the interpreter lock); returns their wall times."""
+    out = [0.0] * len(parts)
+
+    def run(k):
+        out[k] = o1_call(parts[k], cam17, first_seed + k)
+
+    ths = [threading.Thread(target=run, args=(k,)) for k in range(len(parts))]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    return out
+
+
+def cpu_reference(g, cams, threads, stride=64, step=0):
+    """Full-scene seconds per ensemble of each view, all host threads busy. Thread t renders one
+    ensemble of its own uniform 1/stride subset of the splats (subset (step * threads + t) mod
+    stride, disjoint across threads; the generator shuffles splats), so the sample averages over
+    `threads` subsets; the per-ensemble fixed cost a (framebuffer set-up and resolve, measured the
+    same way on one splat) is not multiplied: full = a + stride (mean t - a), and with all threads
+    busy the job renders `threads` such ensembles in that time. Returns (ensembles/s, per-view
+    ms/ensemble, per-view fixed ms, per-view coefficient of variation of the subsets' per-splat
+    times)."""
+    per_view, fixed, spread = {}, {}, {}
+    total = 0.0
+    for name, cam in cams:
+        a = statistics.median(o1_concurrent([g[:1]] * threads, cam, 1))
+        parts = [g[((step * threads + t) % stride)::stride] for t in range(threads)]
+        ts = o1_concurrent(parts, cam, 1 + step * threads)
+        var = [max(t - a, 0.0) for t in ts]
+        mean = statistics.fmean(var)
+        full = a + stride * mean  # one full-scene ensemble on one thread
+        s_per_ens = full / threads
         per_view[name] = 1000.0 * s_per_ens
-        total_s_per_ens += s_per_ens
-    return len(views_cams) / total_s_per_ens, per_view
+        fixed[name] = 1000.0 * a
+        spread[name] = statistics.pstdev(var) / max(mean, 1e-12)
+        total += s_per_ens
+    return len(cams) / total, per_view, fixed, spread
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    pkg = load_package()
-    splats, sh, deg = build_scene(pkg)
-    cams = cameras(pkg)
+    g, cams = reference_inputs()
     threads = os.cpu_count() or 1
-    fraction = args.cpu_fraction
-    for _ in range(args.warmup):
-        cpu_reference(pkg, splats, fraction, threads, cams)
-    rates, views = [], []
+    stride = int(round(1.0 / args.cpu_fraction))
+    for k in range(args.warmup):
+        cpu_reference(g, cams, threads, stride, k)
+    rates, views, fixed, spread = [], [], [], []
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        r, v = cpu_reference(pkg, splats, fraction, threads, cams)
+    for k in range(args.steps):
+        r, v, a, sp = cpu_reference(g, cams, threads, stride, args.warmup + k)
         rates.append(r)
         views.append(v)
+        fixed.append(a)
+        spread.append(sp)
     wall = time.perf_counter() - t0
     value = statistics.median(rates)
-    sample = (f"first {fraction:g} of the {N_SPLATS} splats (uniform subset), {threads} ensembles in parallel "
-              f"(one per thread) per view, time scaled to the full scene")
+    sample = (f"per view {threads} host threads, each rendering one ensemble of its own disjoint 1/{stride} splat "
+              f"subset; full-scene time = fixed per-ensemble cost (measured on one splat) + {stride} x the mean "
+              f"per-splat part; successive steps take the next subsets")
     line = {"impl": "reference", "metric": "ensembles/s (PBVR Ext C3+R, 560k Gaussians SH3, 1280x720, near/mid/far)",
             "value": value, "unit": "ensembles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * wall / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
             "ms_per_ensemble": {k: statistics.median([v[k] for v in views]) for k in views[0]},
+            "fixed_ms_per_call": {k: statistics.median([v[k] for v in fixed]) for k in fixed[0]},
+            "subset_cv": {k: max(v[k] for v in spread) for k in spread[0]},
             "cpu_baseline": {"value": value, "unit": "ensembles/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "ensembles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -612,13 +672,15 @@ def run_b200(args, rank, world):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cams = cameras(pkg)
         threads = os.cpu_count() or 1
-        rate, cpu_views = cpu_reference(pkg, splats, args.cpu_fraction, threads, cams)
+        stride = int(round(1.0 / args.cpu_fraction))
+        rg, rcams = reference_inputs()
+        rate, cpu_views, cpu_fixed, cpu_spread = cpu_reference(rg, rcams, threads, stride, 0)
         cpu = {"value": rate, "unit": "ensembles/s", "cores": threads, "kind": "port",
-               "sample": f"first {args.cpu_fraction:g} of the {N_SPLATS} splats (uniform subset), one ensemble per "
-                         f"thread per view, {threads} threads, time scaled to the full scene",
-               "ms_per_ensemble": cpu_views}
+               "sample": f"per view {threads} host threads, each rendering one ensemble of its own disjoint 1/{stride} "
+                         f"splat subset; full-scene time = fixed per-ensemble cost (measured on one splat) + {stride} x "
+                         f"the mean per-splat part",
+               "ms_per_ensemble": cpu_views, "fixed_ms_per_call": cpu_fixed, "subset_cv": cpu_spread}
 
     if rank == 0:
         line = {"metric": "ensembles/s (PBVR Ext C3+R, 560k Gaussians SH3, 1280x720, near/mid/far)",
@@ -667,7 +729,7 @@ def main():
     ap.add_argument("--stress-res", default="3840x2160")
     ap.add_argument("--stress-cap", type=int, default=65536)
     ap.add_argument("--stress-ref", type=int, default=256, help="ensembles of the stress reference")
-    ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64)
+    ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64, help="splat fraction each host thread renders")
     ap.add_argument("--views", default="near,mid,far", help="subset of the views (small profiling cases)")
     ap.add_argument("--ensembles", type=int, default=ENS, help="ensembles per view (small profiling cases)")
     args = ap.parse_args()

@@ -36,3 +36,25 @@ def test_peak_and_workload():
     cfg = bench.workload_config()
     assert cfg["gaussians"] == bench.N_SPLATS and cfg["resolution"] == [bench.W, bench.H]
     assert cfg["views"] == [v for v, _ in bench.VIEWS] and cfg["ensembles_per_view"] == bench.ENS
+
+
+def test_reference_arm_never_loads_the_renderer():
+    """The CPU arm builds its scene and cameras from the oracle alone (oracle PLY reader, O1
+    cameras equal to the renderer's) and its timing helper runs O1 in one host thread per subset;
+    the renderer library is not mapped into that process."""
+    import subprocess
+    code = ("import sys; sys.path.insert(0, %r); import bench; g, cams = bench.reference_inputs(); "
+            "r = bench.cpu_reference(g[:20000], cams[2:], 2, 64); assert r[0] > 0; "
+            "print(any('libgpsb200' in l for l in open('/proc/self/maps')))" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip().splitlines()[-1] == "False"
+
+
+def test_reference_cameras_equal_the_renderers():
+    import numpy as np
+    from conftest import load_package
+    pkg = load_package()
+    _, cams = bench.reference_inputs()
+    for (name, c17), (name2, cam) in zip(cams, bench.cameras(pkg)):
+        assert name == name2 and np.array_equal(c17, cam.to_array())
