@@ -159,6 +159,9 @@ SIGNATURES = {
     "gpsb_session_read_state": (ST, [P, P]),
     # denoiser kernels (return cudaError_t codes)
     "gpsb_dn_conv_fwd": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, ST, P, P, ST, ST, ST, ST, P, P]),
+    "gpsb_dn_conv3_weight_bytes": (C.c_ulonglong, [ST, ST]),
+    "gpsb_dn_conv3_weights": (ST, [P, ST, ST, ST, P, P]),
+    "gpsb_dn_conv3": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, P, P, ST, ST, ST, ST, P, P]),
     "gpsb_dn_conv_dw": (ST, [P, ST, P, ST, ST, ST, ST, ST, ST, ST, ST, P, P, P]),
     "gpsb_dn_flip": (ST, [P, ST, ST, ST, P, ST, ST, P]),
     "gpsb_dn_relu_bwd": (ST, [P, ST, ST, P, ST, ST, ST, ST, P, ST, P]),

@@ -1,0 +1,503 @@
+// Direct 3x3 convolution (stride 1, zero padding 1) of NHWC bf16 activations on the tcgen05 tensor
+// cores, with every operand staged by TMA: the denoiser's forward layers and the data gradients of
+// its backward pass (the same convolution with flipped weights).
+//
+//   Y[b][y][x][n] = act(bias[n] + sum_{dy,dx,ci} X[b][y+dy][x+dx][ci] W[n][(dy+1)*3 + (dx+1)][ci])
+//
+// Work unit ("block"): R output rows x one 128-pixel row segment of one image, all N output
+// channels. The K loop runs over groups of G input channels. One pipeline stage holds
+//   * the R + 2 input rows y0-1 .. y0+R of pixels x0-1 .. x0+128 of the group's channels, one
+//     plane per 8-channel chunk: [chunk][row][pixel][8 channels], 16 bytes per (row, pixel), loaded
+//     by one TMA box per chunk from a 5-D view (8 channels, chunk, W, H, B) of the activation
+//     tensor; pixels and rows outside the image read as zeros (TMA out-of-bounds fill), which is
+//     the convolution's padding;
+//   * the group's weights in the canonical K-major layout of the MMA's B operand, one 1-D bulk copy
+//     of a block that gpsb_dn_conv3_weights arranged once: [tap][chunk][n][8 channels].
+// In the canonical K-major layout without swizzle a core matrix is 8 rows x 16 bytes, i.e. eight
+// consecutive pixels of one chunk plane; the MMA of output row r, tap (dy, dx) and chunk pair j
+// reads A from plane 2j, row r + dy + 1, starting at pixel dx + 1 (leading byte offset = the plane
+// size, stride byte offset = 128 bytes): the nine taps are nine descriptors over the same staged
+// rows, so each input byte crosses from L2 once per block instead of nine times.
+//
+// Roles (persistent CTAs, one per SM, 192 threads): warp 0 issues the TMA copies, one thread of
+// warp 1 issues the MMAs (M = 128 pixels, N, K = 16) into one of two tensor-memory accumulators of
+// R x N fp32 columns, warps 2-5 read the other accumulator back (tcgen05.ld, warp w reads lanes
+// 32 (w % 4) ..) and apply bias, ReLU and the bf16 / fp32 store, so the epilogue of block i
+// overlaps the MMAs of block i + 1. Stages and accumulators hand over through mbarriers (TMA
+// transaction counts, tcgen05.commit, epilogue arrivals). Every wait is bounded: a wait that gives
+// up sets bit CONV3_ERR_TIMEOUT in the caller's error word and raises an abort flag that ends every
+// role; the CTA then waits (bounded) for its own TMA copies and MMAs before it frees its tensor
+// memory and returns. No cluster, no multicast.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+
+#include "umma.cuh"
+
+namespace gpsb {
+namespace c3 {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kSeg = 128;             // output pixels of a row segment (the MMA's M)
+constexpr int kHalo = kSeg + 2;       // staged input pixels per row
+constexpr int kThreads = 192;         // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr uint32_t kAccCols = 256;    // tensor-memory columns of one accumulator (two are allocated)
+constexpr uint32_t kSpin = 1u << 24;  // polls of a bounded wait
+constexpr uint32_t CONV3_ERR_TIMEOUT = 32u;
+
+__host__ __device__ constexpr int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Per output-channel width N: R rows per block (R x N <= 256 accumulator columns), G channels per
+// stage, S stages, and the byte layout of a stage.
+template <int N>
+struct Cfg {
+    static constexpr int R = N <= 32 ? 8 : N <= 64 ? 4 : N <= 128 ? 2 : 1;
+    static constexpr int G = N >= 192 ? 16 : 32;
+    static constexpr int CH = G / 8;                                     // chunk planes per stage
+    static constexpr int BOX = (R + 2) * kHalo * 16;                     // bytes one TMA box writes
+    static constexpr int PLANE = round_up(BOX, 128);                     // plane stride in shared memory
+    static constexpr int IN = CH * PLANE;
+    static constexpr int WB = 9 * CH * N * 16;                           // weight bytes of one group
+    static constexpr int STAGE = round_up(IN + WB, 1024);
+    static constexpr int S = N >= 192 ? 3 : 2;
+    static constexpr uint32_t TX = (uint32_t)(CH * BOX + WB);            // bytes landing per stage
+    static constexpr size_t SMEM = (size_t)S * STAGE + 1024;             // + alignment slack
+    static_assert(R * N <= (int)kAccCols, "accumulator columns");
+    static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N of one MMA");
+    static_assert(SMEM <= 232448, "shared memory per CTA");
+};
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor, K-major, no swizzle (sm_100 descriptor version 1)
+__device__ __forceinline__ uint64_t desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void bar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool bar_test(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase of parity `parity`; gives up when the limit passes or another role
+// raised the abort flag.
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, volatile int* abort) {
+    for (uint32_t i = 0; i < kSpin; ++i) {
+        if (bar_test(b, parity)) return true;
+        if ((i & 255u) == 255u && *abort) return false;
+    }
+    return false;
+}
+__device__ __forceinline__ void bar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+__device__ __forceinline__ void bar_expect(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+// one 5-D TMA tile load into shared memory, completion counted on the mbarrier
+__device__ __forceinline__ void tma_load5(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                          uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(saddr(bar))
+        : "memory");
+}
+// one contiguous bulk copy global -> shared (16-byte aligned, size a multiple of 16)
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(saddr(bar))
+                 : "memory");
+}
+
+struct Params {
+    const bf16* wt;       // arranged weights: [group][tap][chunk][n][8]
+    const float* bias;    // [cout] or null
+    void* out;            // [B][H][W][ldo] at channel offset ooff, bf16 or fp32
+    int ldo, ooff, out_f32, relu;
+    int B, H, W, cout, groups;
+    int segs, rowblocks, blocks;
+    uint32_t* err;
+};
+
+template <int N>
+__global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ CUtensorMap xmap, const Params p) {
+    using C = Cfg<N>;
+    extern __shared__ __align__(1024) uint8_t s_raw[];
+    __shared__ __align__(8) uint64_t s_full[C::S], s_empty[C::S], s_acc_full[2], s_acc_empty[2], s_drain;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_abort;
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_raw) + 1023) & ~(uintptr_t)1023);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&s_tmem)),
+                     "r"(2u * kAccCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 32) {
+        for (int s = 0; s < C::S; ++s) {
+            bar_init(&s_full[s], 1);
+            bar_init(&s_empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            bar_init(&s_acc_full[a], 1);
+            bar_init(&s_acc_empty[a], 4);
+        }
+        bar_init(&s_drain, 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+
+    auto fail = [&]() {
+        if (!s_abort) {
+            s_abort = 1;
+            atomicOr(p.err, CONV3_ERR_TIMEOUT);
+        }
+    };
+    // block -> (image, first output row, first output pixel)
+    auto decode = [&](int blk, int& b, int& y0, int& x0) {
+        const int seg = blk % p.segs, rb = (blk / p.segs) % p.rowblocks;
+        b = blk / (p.segs * p.rowblocks);
+        y0 = rb * C::R;
+        x0 = seg * kSeg;
+    };
+
+    if (warp == 0) {
+        // ------------------------------------------------------------------ TMA producer
+        uint32_t armed = 0;  // stages armed at least once (for the abort drain)
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
+            int stage = 0;
+            uint32_t phase = 0;
+            for (int blk = blockIdx.x; blk < p.blocks && !s_abort; blk += gridDim.x) {
+                int b, y0, x0;
+                decode(blk, b, y0, x0);
+                for (int g = 0; g < p.groups; ++g) {
+                    if (!bar_wait(&s_empty[stage], phase ^ 1u, &s_abort)) {
+                        fail();
+                        break;
+                    }
+                    uint8_t* st = base + (size_t)stage * C::STAGE;
+                    bar_expect(&s_full[stage], C::TX);
+                    for (int c = 0; c < C::CH; ++c)
+                        tma_load5(saddr(st + c * C::PLANE), &xmap, 0, g * C::CH + c, x0 - 1, y0 - 1, b, &s_full[stage]);
+                    bulk_load(saddr(st + C::IN), p.wt + (size_t)g * (C::WB / 2), (uint32_t)C::WB, &s_full[stage]);
+                    armed |= 1u << stage;
+                    if (++stage == C::S) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            if (s_abort) {
+                // let this CTA's copies land before the CTA can exit: every stage's last armed phase
+                // completes by its transaction count alone
+                int st2 = stage;
+                uint32_t ph2 = phase;
+                for (int k = 0; k < C::S; ++k) {
+                    if (--st2 < 0) {
+                        st2 = C::S - 1;
+                        ph2 ^= 1u;
+                    }
+                    if (armed & (1u << st2)) {
+                        for (uint32_t i = 0; i < kSpin && !bar_test(&s_full[st2], ph2); ++i) {
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            constexpr uint32_t idesc = umma::idesc_bf16(N);
+            int stage = 0, a = 0;
+            uint32_t phase = 0, aphase = 0;
+            bool issued = false;
+            for (int blk = blockIdx.x; blk < p.blocks && !s_abort; blk += gridDim.x) {
+                if (!bar_wait(&s_acc_empty[a], aphase ^ 1u, &s_abort)) {
+                    fail();
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)a * kAccCols;
+                bool ok = true;
+                for (int g = 0; g < p.groups; ++g) {
+                    if (!bar_wait(&s_full[stage], phase, &s_abort)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t st = saddr(base + (size_t)stage * C::STAGE);
+                    const uint32_t wb = st + C::IN;
+#pragma unroll 1
+                    for (int r = 0; r < C::R; ++r) {
+#pragma unroll
+                        for (int t = 0; t < 9; ++t) {
+                            const int dy = t / 3, dx = t % 3;  // input row r + dy, pixel offset dx (staged from -1)
+#pragma unroll
+                            for (int j = 0; j < C::CH / 2; ++j) {
+                                const uint32_t aa = st + (uint32_t)(2 * j) * C::PLANE + (uint32_t)((r + dy) * kHalo + dx) * 16u;
+                                const uint32_t bb = wb + (uint32_t)((t * C::CH + 2 * j) * N) * 16u;
+                                umma::mma_bf16(acc + (uint32_t)(r * N), desc(aa, C::PLANE, 128), desc(bb, N * 16, 128),
+                                               idesc, g > 0 || t > 0 || j > 0);
+                            }
+                        }
+                    }
+                    umma::mma_commit(&s_empty[stage]);  // frees the stage when these MMAs complete
+                    issued = true;
+                    if (++stage == C::S) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) {
+                    fail();
+                    break;
+                }
+                umma::mma_commit(&s_acc_full[a]);
+                if (++a == 2) {
+                    a = 0;
+                    aphase ^= 1u;
+                }
+            }
+            // every MMA this CTA issued has completed before its tensor memory can be freed
+            if (issued) {
+                umma::mma_commit(&s_drain);
+                for (uint32_t i = 0; i < kSpin && !bar_test(&s_drain, 0); ++i) {
+                }
+            }
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------------ epilogue (warps 2-5)
+        const int quad = warp & 3;  // tensor-memory lanes 32 quad ..
+        const int px = quad * 32 + lane;
+        int a = 0;
+        uint32_t aphase = 0;
+        for (int blk = blockIdx.x; blk < p.blocks && !s_abort; blk += gridDim.x) {
+            int b, y0, x0;
+            decode(blk, b, y0, x0);
+            if (!bar_wait(&s_acc_full[a], aphase, &s_abort)) {
+                fail();
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int x = x0 + px;
+            const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)a * kAccCols;
+#pragma unroll 1
+            for (int r = 0; r < C::R; ++r) {
+                const int y = y0 + r;
+                const bool valid = x < p.W && y < p.H;
+                const size_t o = (((size_t)b * p.H + (valid ? y : 0)) * p.W + (valid ? x : 0)) * p.ldo + p.ooff;
+#pragma unroll 1
+                for (int c = 0; c < N; c += 16) {
+                    float v[16];
+                    umma::tmem_ld16(lane_base + (uint32_t)(r * N + c), v);  // every lane: .sync.aligned
+                    if (!valid) continue;
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int n = c + k;
+                        float s = v[k] + ((p.bias && n < p.cout) ? __ldg(&p.bias[n]) : 0.0f);
+                        v[k] = p.relu ? fmaxf(s, 0.0f) : s;
+                    }
+                    if (c + 16 <= p.cout && ((p.ldo | p.ooff) & 7) == 0) {
+                        if (p.out_f32) {
+                            float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(p.out) + o + c);
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                        } else {
+                            uint32_t w[8];
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) {
+                                __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                                w[q] = *reinterpret_cast<uint32_t*>(&h);
+                            }
+                            uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(p.out) + o + c);
+                            dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                            dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) {
+                            if (c + k < p.cout) {
+                                if (p.out_f32) reinterpret_cast<float*>(p.out)[o + c + k] = v[k];
+                                else reinterpret_cast<bf16*>(p.out)[o + c + k] = __float2bfloat16_rn(v[k]);
+                            }
+                        }
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) bar_arrive(&s_acc_empty[a]);
+            if (++a == 2) {
+                a = 0;
+                aphase ^= 1u;
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2u * kAccCols) : "memory");
+}
+
+// Weights of one layer in the order the kernel streams them: wt[g][t][c][n][e] = w[n][t * cin + g G + 8 c + e]
+// (zero past cin or cout). w: [cout][kp] bf16, K index k = tap * cin + ci.
+__global__ void k_conv3_arrange(const bf16* w, int cout, int cin, int kp, int N, int G, int groups, bf16* wt) {
+    const int CH = G / 8;
+    const long total = (long)groups * 9 * CH * N * 8;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        long q = i;
+        const int e = (int)(q % 8);
+        q /= 8;
+        const int n = (int)(q % N);
+        q /= N;
+        const int c = (int)(q % CH);
+        q /= CH;
+        const int t = (int)(q % 9);
+        const int g = (int)(q / 9);
+        const int ci = g * G + c * 8 + e;
+        bf16 v = __float2bfloat16_rn(0.0f);
+        if (n < cout && ci < cin) v = w[(size_t)n * kp + t * cin + ci];
+        wt[i] = v;
+    }
+}
+
+// N of the kernel instance serving `cout` output channels
+static int n_of(int cout) {
+    if (cout <= 16) return 16;
+    if (cout <= 32) return 32;
+    if (cout <= 64) return 64;
+    if (cout <= 96) return 96;
+    if (cout <= 128) return 128;
+    return 192;
+}
+static int g_of(int N) { return N >= 192 ? 16 : 32; }
+
+static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    return fn;
+}
+
+template <int N>
+static cudaError_t launch(const bf16* x, int ldx, int xoff, int cin, const Params& prm, cudaStream_t st) {
+    using Cf = Cfg<N>;
+    auto enc = encoder();
+    if (!enc) return cudaErrorNotSupported;
+    // 5-D view of the activations: (8 channels, chunk, W, H, B); channel chunks of [xoff, xoff + cin)
+    CUtensorMap map;
+    const cuuint64_t dims[5] = {8, (cuuint64_t)((cin + 7) / 8), (cuuint64_t)prm.W, (cuuint64_t)prm.H, (cuuint64_t)prm.B};
+    const cuuint64_t strides[4] = {16, (cuuint64_t)ldx * 2, (cuuint64_t)prm.W * ldx * 2, (cuuint64_t)prm.H * prm.W * ldx * 2};
+    const cuuint32_t box[5] = {8, 1, (cuuint32_t)kHalo, (cuuint32_t)(Cf::R + 2), 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)(x + xoff), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    Params q = prm;
+    q.segs = (prm.W + kSeg - 1) / kSeg;
+    q.rowblocks = (prm.H + Cf::R - 1) / Cf::R;
+    q.blocks = q.segs * q.rowblocks * prm.B;
+    q.groups = (cin + Cf::G - 1) / Cf::G;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaFuncSetAttribute(k_conv3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cf::SMEM);
+    if (e != cudaSuccess) return e;
+    const int grid = q.blocks < sms ? q.blocks : sms;
+    if (grid <= 0) return cudaSuccess;
+    k_conv3<N><<<grid, kThreads, Cf::SMEM, st>>>(map, q);
+    return cudaGetLastError();
+}
+
+}  // namespace c3
+}  // namespace gpsb
+
+using namespace gpsb;
+using namespace gpsb::c3;
+
+extern "C" {
+
+// Bytes of the arranged weights of a layer with cout outputs and cin inputs (see k_conv3_arrange).
+unsigned long long gpsb_dn_conv3_weight_bytes(int cout, int cin) {
+    if (cout < 1 || cout > 192 || cin < 1) return 0;
+    const int N = n_of(cout), G = g_of(N);
+    return (unsigned long long)((cin + G - 1) / G) * 9ull * (G / 8) * N * 16ull;
+}
+
+// Arranges w ([cout][kp] bf16, k = tap * cin + ci) into wt (gpsb_dn_conv3_weight_bytes bytes).
+int gpsb_dn_conv3_weights(const void* w, int cout, int cin, int kp, void* wt, void* stream) {
+    if (cout < 1 || cout > 192 || cin < 1 || kp < 9 * cin || !w || !wt) return (int)cudaErrorInvalidValue;
+    const int N = n_of(cout), G = g_of(N), groups = (cin + G - 1) / G;
+    const long total = (long)groups * 9 * (G / 8) * N * 8;
+    const int blocks = (int)((total + 255) / 256 < 1184 ? (total + 255) / 256 : 1184);
+    k_conv3_arrange<<<blocks, 256, 0, (cudaStream_t)stream>>>((const bf16*)w, cout, cin, kp, N, G, groups, (bf16*)wt);
+    return (int)cudaGetLastError();
+}
+
+// 3x3 convolution, stride 1, zero padding 1: NHWC bf16 input x (B, H, W, ldx) channels
+// [xoff, xoff + cin), arranged weights wt, output (B, H, W, ldo) channels [ooff, ooff + cout),
+// bf16 or fp32 (out_f32), optional bias and ReLU. ldx and xoff multiples of 8, x 16-byte aligned,
+// cout <= 192. Enqueues on `stream`; a device-side wait that gives up sets bit 32 of *err.
+int gpsb_dn_conv3(const void* x, int ldx, int xoff, int cin, int B, int H, int W, const void* wt, int cout,
+                  const float* bias, void* out, int ldo, int ooff, int out_f32, int relu, void* stream, uint32_t* err) {
+    if (!x || !wt || !out || !err || ldx % 8 || xoff % 8 || cin < 1 || xoff + cin > ldx || cout < 1 || cout > 192 ||
+        B < 1 || H < 1 || W < 1 || ooff < 0 || ooff + cout > ldo || (reinterpret_cast<uintptr_t>(x) & 15u))
+        return (int)cudaErrorInvalidValue;
+    Params prm{};
+    prm.wt = (const bf16*)wt;
+    prm.bias = bias;
+    prm.out = out;
+    prm.ldo = ldo;
+    prm.ooff = ooff;
+    prm.out_f32 = out_f32;
+    prm.relu = relu;
+    prm.B = B;
+    prm.H = H;
+    prm.W = W;
+    prm.cout = cout;
+    prm.err = err;
+    const bf16* xb = (const bf16*)x;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (n_of(cout)) {
+        case 16: return (int)launch<16>(xb, ldx, xoff, cin, prm, st);
+        case 32: return (int)launch<32>(xb, ldx, xoff, cin, prm, st);
+        case 64: return (int)launch<64>(xb, ldx, xoff, cin, prm, st);
+        case 96: return (int)launch<96>(xb, ldx, xoff, cin, prm, st);
+        case 128: return (int)launch<128>(xb, ldx, xoff, cin, prm, st);
+        default: return (int)launch<192>(xb, ldx, xoff, cin, prm, st);
+    }
+}
+
+}  // extern "C"

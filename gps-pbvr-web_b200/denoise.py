@@ -1,6 +1,7 @@
 """Learned denoiser of few-ensemble accumulations: a 3-level U-Net of 3x3 convolutions whose
-forward and backward passes run on the library's tcgen05 kernels (csrc/denoise.cu), with BF16
-weights and activations and FP32 accumulation. PyTorch tensors only hold device memory here.
+forward and backward passes run on the library's tcgen05 kernels (csrc/conv3x3.cu for the
+convolutions and data gradients, csrc/denoise.cu for the weight gradients and element-wise steps),
+with BF16 weights and activations and FP32 accumulation. PyTorch tensors only hold device memory here.
 """
 import ctypes as C
 import os
@@ -37,6 +38,26 @@ def conv_fwd(x, cin, w, cout, bias, out, *, xoff=0, ooff=0, relu=False, err):
                                    ooff, int(out.dtype == torch.float32), int(relu), _stream(), _p(err)), "conv_fwd")
 
 
+def conv3_weights(w, cout, cin, wt=None):
+    """Weights w (cout, kp) bf16 arranged for conv3 into wt (a uint8 CUDA tensor, allocated when None)."""
+    import torch
+    L = abi.lib()
+    n = int(L.gpsb_dn_conv3_weight_bytes(cout, cin))
+    if wt is None or wt.numel() != n:
+        wt = torch.zeros(n, dtype=torch.uint8, device=w.device)
+    _ck(L.gpsb_dn_conv3_weights(_p(w), cout, cin, w.shape[1], _p(wt), _stream()), "conv3_weights")
+    return wt
+
+
+def conv3(x, cin, wt, cout, bias, out, *, xoff=0, ooff=0, relu=False, err):
+    """conv_fwd on the TMA-staged engine, with weights arranged by conv3_weights."""
+    import torch
+    B, H, W, ldx = x.shape
+    ldo = out.shape[-1]
+    _ck(abi.lib().gpsb_dn_conv3(_p(x), ldx, xoff, cin, B, H, W, _p(wt), cout, _p(bias), _p(out), ldo, ooff,
+                                int(out.dtype == torch.float32), int(relu), _stream(), _p(err)), "conv3")
+
+
 def conv_dw(dy, x, cin, cout, dw, *, xoff=0, err):
     """dw (cout, kp) fp32 += weight gradient of the convolution of x channels [xoff, xoff + cin)
     given the bf16 output gradient dy (B, H, W, ldy)."""
@@ -70,8 +91,13 @@ class Denoiser:
     to the few-ensemble mean colour. Master weights fp32 (Adam state beside them), compute copies
     bf16; every arithmetic step runs in the library's kernels."""
 
-    def __init__(self, seed=0, device="cuda"):
+    def __init__(self, seed=0, device="cuda", engine="tma"):
+        """engine: "tma" runs the convolutions and data gradients on conv3 (TMA-staged operands),
+        "cp.async" on the earlier implicit-im2col kernels (kept for comparison)."""
         import torch
+        if engine not in ("tma", "cp.async"):
+            raise ValueError("engine must be 'tma' or 'cp.async'")
+        self.engine = engine
         self.device = torch.device(device)
         g = torch.Generator().manual_seed(seed)
         self.p = {}
@@ -106,6 +132,9 @@ class Denoiser:
         for q in self.p.values():
             _ck(_L().gpsb_dn_to_bf16(_p(q["w"]), q["kp"], q["cout"], q["kp"], _p(q["wb"]), q["kp"], st), "to_bf16")
             flip(q["wb"], q["cout"], q["cin"], q["wf"], q["coutp"])
+            if self.engine == "tma":
+                q["wt"] = conv3_weights(q["wb"], q["cout"], q["cin"], q.get("wt"))
+                q["wft"] = conv3_weights(q["wf"], q["cin"], q["coutp"], q.get("wft"))
 
     def state_dict(self):
         return {n: {"w": q["w"].cpu(), "b": q["b"].cpu()} for n, q in self.p.items()}
@@ -169,7 +198,10 @@ class Denoiser:
     # ------------------------------------------------------------------ forward
     def _conv(self, name, x, out, *, xoff=0, ooff=0, relu=True):
         q = self.p[name]
-        conv_fwd(x, q["cin"], q["wb"], q["cout"], q["b"], out, xoff=xoff, ooff=ooff, relu=relu, err=self.err)
+        if self.engine == "tma":
+            conv3(x, q["cin"], q["wt"], q["cout"], q["b"], out, xoff=xoff, ooff=ooff, relu=relu, err=self.err)
+        else:
+            conv_fwd(x, q["cin"], q["wb"], q["cout"], q["b"], out, xoff=xoff, ooff=ooff, relu=relu, err=self.err)
 
     def forward(self, x0, base):
         """x0 (B, H, W, 8) bf16 features, base (B, H, W, 3) fp32 mean colour -> prediction (B, H, W, 3)."""
@@ -203,7 +235,10 @@ class Denoiser:
         conv_dw(dz, x, q["cin"], q["cout"], q["gw"], xoff=xoff, err=self.err)
         _ck(_L().gpsb_dn_bias_grad(_p(dz), dz.shape[-1], B * H * W, q["cout"], _p(q["gb"]), _stream()), "bias_grad")
         if data_grad:
-            conv_fwd(dz, q["coutp"], q["wf"], q["cin"], None, gx, err=self.err)
+            if self.engine == "tma":
+                conv3(dz, q["coutp"], q["wft"], q["cin"], None, gx, err=self.err)
+            else:
+                conv_fwd(dz, q["coutp"], q["wf"], q["cin"], None, gx, err=self.err)
 
     def _relu_bwd(self, g, ldg, goff, y, ldy, yoff, C, out):
         B, H, W, ldo = out.shape

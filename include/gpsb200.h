@@ -429,6 +429,17 @@ gpsb_status gpsb_session_read_state(const gpsb_session* s, gpsb_session_state* o
 int gpsb_dn_conv_fwd(const void* x, int ldx, int xoff, int cin, int B, int H, int W, const void* w, int cout,
                      int kp, const float* bias, void* out, int ldo, int ooff, int out_f32, int relu,
                      void* stream, uint32_t* err);
+/* The same convolution with TMA-staged operands (persistent, warp-specialised CTAs: the input rows
+ * of an R-row x 128-pixel block are staged once as 8-channel planes and the nine taps are shifted
+ * shared-memory descriptors over them; two tensor-memory accumulators overlap the epilogue with the
+ * next block's MMAs). Weights come pre-arranged by gpsb_dn_conv3_weights into a buffer of
+ * gpsb_dn_conv3_weight_bytes(cout, cin) bytes. x 16-byte aligned, ldx and xoff multiples of 8,
+ * cout <= 192; a bounded device-side wait that gives up sets bit 32 of *err (err required). */
+unsigned long long gpsb_dn_conv3_weight_bytes(int cout, int cin);
+int gpsb_dn_conv3_weights(const void* w, int cout, int cin, int kp, void* wt, void* stream);
+int gpsb_dn_conv3(const void* x, int ldx, int xoff, int cin, int B, int H, int W, const void* wt, int cout,
+                  const float* bias, void* out, int ldo, int ooff, int out_f32, int relu, void* stream,
+                  uint32_t* err);
 /* dw[co][k] += sum_p dy[p][co] * xcol[p][k] (fp32, caller-zeroed): the weight gradient. */
 int gpsb_dn_conv_dw(const void* dy, int ldy, const void* x, int ldx, int xoff, int cin, int B, int H, int W,
                     int cout, int kp, float* dw, void* stream, uint32_t* err);
