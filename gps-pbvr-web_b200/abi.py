@@ -160,6 +160,16 @@ SIGNATURES = {
     # denoiser kernels (return cudaError_t codes)
     "gpsb_dn_conv_fwd": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, ST, P, P, ST, ST, ST, ST, P, P]),
     "gpsb_dn_conv3_weight_bytes": (C.c_ulonglong, [ST, ST]),
+    "gpsb_dn_channel_sum": (ST, [P, ST, ST, ST, P, P]),
+    "gpsb_dn_mean_rgb": (ST, [P, ST, P, P]),
+    "gpsb_denoiser_create": (ST, [ST, P]),
+    "gpsb_denoiser_destroy": (None, [P]),
+    "gpsb_denoiser_last_error": (C.c_char_p, [P]),
+    "gpsb_denoiser_layer_shape": (ST, [U32, P, P, P]),
+    "gpsb_denoiser_set_layer": (ST, [P, U32, P, P]),
+    "gpsb_denoiser_set_gate": (ST, [P, C.c_float]),
+    "gpsb_denoiser_forward": (ST, [P, P, P, U32, U32, P, P]),
+    "gpsb_render_denoised": (ST, [P, P, P, P, U32, U32, C.c_float, U32, P, P, P]),
     "gpsb_dn_conv3_weights": (ST, [P, ST, ST, ST, P, P]),
     "gpsb_dn_conv3": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, P, P, ST, ST, ST, ST, P, P]),
     "gpsb_dn_conv_dw": (ST, [P, ST, P, ST, ST, ST, ST, ST, ST, ST, ST, P, P, P]),

@@ -24,7 +24,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
              "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
 # extra nvcc flags for tuning builds (e.g. GPSB_NVCC_EXTRA="-DGPSB_SORT_LOOKAHEAD=16"; rebuild with --force)
 CU_FLAGS += os.environ.get("GPSB_NVCC_EXTRA", "").split()
-LIB_SOURCES = ["kernels.cu", "sorted.cu", "primitives.cu", "denoise.cu", "conv3x3.cu", "ply_gpu.cu", "renderer.cpp", "session.cpp", "hostmath.cpp", "ply.cpp"]
+LIB_SOURCES = ["kernels.cu", "sorted.cu", "primitives.cu", "denoise.cu", "conv3x3.cu", "ply_gpu.cu", "renderer.cpp", "denoiser.cpp", "session.cpp", "hostmath.cpp", "ply.cpp"]
 
 
 def _headers():

@@ -384,6 +384,23 @@ __global__ void k_crop(const bf16* x, const float* base, const float* target, in
         targetb[(size_t)i * 3 + c] = target[src * 3 + c];
     }
 }
+// *sum += sum over M pixels of channel c of the bf16 tensor x (M x ld): one partial per warp
+__global__ void k_channel_sum(const bf16* x, int ld, int c, int M, float* sum) {
+    float s = 0.0f;
+    for (int m = gtid(); m < M; m += gridDim.x * blockDim.x) s += __bfloat162float(x[(size_t)m * ld + c]);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0 && s != 0.0f) atomicAdd(sum, s);
+}
+// rgb (P x 3) = accumulated colour / max(count, 1) of the renderer's accumulation (P float4)
+__global__ void k_mean_rgb(const float4* accum, int P, float* rgb) {
+    const int p = gtid();
+    if (p >= P) return;
+    const float4 a = accum[p];
+    const float n = fmaxf(a.w, 1.0f);
+    rgb[(size_t)p * 3 + 0] = a.x / n;
+    rgb[(size_t)p * 3 + 1] = a.y / n;
+    rgb[(size_t)p * 3 + 2] = a.z / n;
+}
 }  // namespace dn
 }  // namespace gpsb
 
@@ -508,6 +525,16 @@ int gpsb_dn_to_bf16(const float* src, int lds, int rows, int cols, void* dst, in
 }
 int gpsb_dn_pack(const void* accum, const float* feat, int P, void* x, float* base, void* stream) {
     k_pack<<<grid_of(P), 256, 0, (cudaStream_t)stream>>>((const float4*)accum, feat, P, (bf16*)x, base);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_channel_sum(const void* x, int ld, int c, int M, float* sum, void* stream) {
+    if (c < 0 || c >= ld || M < 0) return (int)cudaErrorInvalidValue;
+    const int blocks = grid_of(M) < 1184 ? grid_of(M) : 1184;
+    if (blocks > 0) k_channel_sum<<<blocks, 256, 0, (cudaStream_t)stream>>>((const bf16*)x, ld, c, M, sum);
+    return (int)cudaGetLastError();
+}
+int gpsb_dn_mean_rgb(const void* accum, int P, float* rgb, void* stream) {
+    if (P > 0) k_mean_rgb<<<grid_of(P), 256, 0, (cudaStream_t)stream>>>((const float4*)accum, P, rgb);
     return (int)cudaGetLastError();
 }
 int gpsb_dn_crop(const void* x, const float* base, const float* target, int N, int H, int W, const int* crops, int B,

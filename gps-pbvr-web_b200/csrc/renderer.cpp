@@ -115,6 +115,12 @@ struct gpsb_renderer {
     uint64_t scene_gen = 0;
 };
 
+namespace gpsb {
+// the renderer's stream and device, for the denoiser host code in this library
+cudaStream_t renderer_stream(gpsb_renderer* r) { return r->stream; }
+int renderer_device(gpsb_renderer* r) { return r->device; }
+}  // namespace gpsb
+
 // Brackets the kernels of one stage with CUDA events on the renderer's stream (when profiling)
 // and counts the kernels launched.
 struct StageScope {

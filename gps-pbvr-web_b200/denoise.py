@@ -374,3 +374,55 @@ def render_denoised(renderer, net, cam, params, first_seed, *, ensembles=4, gate
     renderer.render_ensembles(cam, params, first_seed + ensembles, fallback_ensembles - ensembles)
     acc = torch.from_numpy(renderer.read_accum()).cuda()
     return acc[:, :3] / acc[:, 3:4].clamp(min=1.0), False, check
+
+
+class NativeDenoiser:
+    """The C-ABI denoiser (gpsb_denoiser_*): the same network sequenced by the library's C++ host
+    code, as a Rust or C caller uses it; loaded from the committed weight file."""
+
+    def __init__(self, path=WEIGHTS, device=0):
+        import numpy as np
+        L = abi.lib()
+        h = C.c_void_p()
+        _ck(L.gpsb_denoiser_create(device, C.byref(h)), "gpsb_denoiser_create")
+        self._h, self._L = h, L
+        z = np.load(path)
+        for i, (name, cin, _, cout) in enumerate(LAYERS):
+            w = np.ascontiguousarray(z[f"{name}.w"], np.float32).reshape(cout, 9 * cin)
+            b = np.ascontiguousarray(z[f"{name}.b"], np.float32)
+            self._check(L.gpsb_denoiser_set_layer(h, i, w.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p)))
+        self.gate_limit = float(z["gate_limit"])
+        self._check(L.gpsb_denoiser_set_gate(h, self.gate_limit))
+
+    def _check(self, st):
+        if st != 0:
+            raise RuntimeError(f"denoiser status {st}: {self._L.gpsb_denoiser_last_error(self._h).decode()}")
+
+    def forward(self, x, base, pred):
+        """x (1, H, W, 8) bf16, base (1, H, W, 3) fp32 -> pred (1, H, W, 3) fp32 (CUDA tensors)."""
+        H, W = x.shape[1], x.shape[2]
+        self._check(self._L.gpsb_denoiser_forward(self._h, _p(x), _p(base), W, H, _p(pred), _stream()))
+
+    def render(self, renderer, cam, params, first_seed, ensembles=4, gate_limit=0.0, fallback_ensembles=64):
+        """gpsb_render_denoised: returns (rgb (H*W, 3) float32 numpy array, used_denoiser, check)."""
+        import numpy as np
+        w, h = renderer.size()
+        rgb = np.zeros((w * h, 3), np.float32)
+        used = C.c_int()
+        chk = C.c_float()
+        cc, pc = cam.to_c(), params.to_c()
+        self._check(self._L.gpsb_render_denoised(renderer.handle, self._h, C.byref(cc), C.byref(pc), first_seed,
+                                                 ensembles, gate_limit, fallback_ensembles,
+                                                 rgb.ctypes.data_as(C.c_void_p), C.byref(used), C.byref(chk)))
+        return rgb, bool(used.value), float(chk.value)
+
+    def close(self):
+        if self._h:
+            self._L.gpsb_denoiser_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

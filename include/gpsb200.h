@@ -475,6 +475,40 @@ int gpsb_dn_pack(const void* accum, const float* feat, int P, void* x, float* ba
 int gpsb_dn_crop(const void* x, const float* base, const float* target, int N, int H, int W, const int* crops,
                  int B, int ch, int cw, void* xb, float* baseb, float* targetb, void* stream, uint32_t* err);
 
+/* The denoised frame (no counterpart in the reference, which has no denoiser): the U-Net above,
+ * sequenced on the host in C++ over these kernels, as one object with its weights and buffers.
+ * Layers 0..10 are c1a c1b c2a c2b c3a c3b c4a c4b c5a c5b c6; gpsb_denoiser_layer_shape gives
+ * each layer's padded and real input channels and its outputs. */
+#define GPSB_DN_LAYERS 11
+typedef struct gpsb_denoiser gpsb_denoiser;
+gpsb_status gpsb_denoiser_create(int device, gpsb_denoiser** out);
+void gpsb_denoiser_destroy(gpsb_denoiser* d);
+const char* gpsb_denoiser_last_error(const gpsb_denoiser* d);
+gpsb_status gpsb_denoiser_layer_shape(uint32_t layer, uint32_t* cin, uint32_t* cin_real, uint32_t* cout);
+/* Host weights of one layer: w (cout x 9*cin floats, k = (ky*3 + kx)*cin + ci, cin the padded input
+ * width) and b (cout floats): the "<name>.w" / "<name>.b" arrays of the committed weight file. */
+gpsb_status gpsb_denoiser_set_layer(gpsb_denoiser* d, uint32_t layer, const float* w, const float* b);
+/* The variance-check limit stored with the weights (mean per-pixel ensemble standard deviation). */
+gpsb_status gpsb_denoiser_set_gate(gpsb_denoiser* d, float gate_limit);
+/* The network on device tensors: x (width*height x 8 bf16 features of gpsb_dn_pack), base
+ * (x 3 fp32 mean colour) -> pred_dev (x 3 fp32). Width and height multiples of 4. Synchronous. */
+gpsb_status gpsb_denoiser_forward(gpsb_denoiser* d, const void* x_dev, const float* base_dev, uint32_t width,
+                                  uint32_t height, float* pred_dev, void* cuda_stream);
+/* A denoised frame of renderer r (render_ensembles, crates/gps-render/src/gps.rs:861, followed by
+ * the network): resets r's accumulation, renders `ensembles` ensembles (seeds first_seed..) with
+ * per-pixel feature sums, packs the 8 input features and computes the variance check. When the
+ * check is at most gate_limit (<= 0: the limit set with gpsb_denoiser_set_gate) the network's
+ * prediction is returned (*used_denoiser = 1); otherwise the frame falls back to the plain
+ * accumulation of fallback_ensembles ensembles (the next seeds are added to the same history;
+ * *used_denoiser = 0). rgb_host: width*height*3 floats, linear RGB; *check: the check value.
+ * Runs on r's stream and returns when the frame is in rgb_host. */
+gpsb_status gpsb_render_denoised(gpsb_renderer* r, gpsb_denoiser* d, const gpsb_camera* cam, const gpsb_params* p,
+                                 uint32_t first_seed, uint32_t ensembles, float gate_limit,
+                                 uint32_t fallback_ensembles, float* rgb_host, int* used_denoiser, float* check);
+/* Sum of channel c of a bf16 tensor (M x ld) added into *sum; rgb (P x 3) = accumulation / count. */
+int gpsb_dn_channel_sum(const void* x, int ld, int c, int M, float* sum, void* stream);
+int gpsb_dn_mean_rgb(const void* accum, int P, float* rgb, void* stream);
+
 /* ------------------------------------------------------------------- PLY (gps-io) */
 /* load_ply (crates/gps-io/src/lib.rs:260-338) + activation (lib.rs:84-96) +
  * GpuGaussian::from_activated (gps.rs:41-49), parsed on the host. Two calls: first with
