@@ -107,32 +107,59 @@ def psnr(a, b):
     return (99.0 if mse == 0 else 10.0 * math.log10(1.0 / mse)), float((a - b).abs().max())
 
 
-def make_frames(pkg, fr, scene_specs, cams_per_scene, in_ens, tgt_ens, rng, seed_base):
-    """Stacked training/evaluation frames: x (N, H, W, 8) bf16, base and target (N, H, W, 3)."""
+def make_frames(pkg, fr, scene_specs, cams_per_scene, in_ens, tgt_ens, rng, seed_base, time_budget_s=None,
+                log=None):
+    """Stacked training frames: x (N, H, W, 8) bf16, base and target (N, H, W, 3) fp32, filled in
+    place in tensors allocated once (N = scenes x cameras) and trimmed to the frames rendered when
+    the optional time budget runs out. Each frame: `in_ens` ensembles with feature sums packed by
+    gpsb_dn_pack straight from the renderer's accumulation, and the mean colour of `tgt_ens`
+    ensembles with disjoint seeds (gpsb_dn_mean_rgb), both on the device."""
     import torch
     from gps_pbvr_web_b200 import denoise as dn
     from gps_pbvr_web_b200 import scenes
     W, H = fr.W, fr.H
     P = W * H
     p = params(pkg)
-    xs, bases, tgts, meta = [], [], [], []
+    N = len(scene_specs) * cams_per_scene
+    xs = torch.zeros(N, H, W, 8, dtype=torch.bfloat16, device="cuda")
+    bases = torch.zeros(N, H, W, 3, device="cuda")
+    tgts = torch.zeros(N, H, W, 3, device="cuda")
+    meta = []
     k = 0
+    t0 = time.perf_counter()
+    L = pkg.abi.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    fr.r.set_stream(stream)
+    acc = fr.r.accum_device_ptr()
+    import ctypes as C
     for n_splats, sseed in scene_specs:
         splats, sh, deg = pkg.load_ply(scenes.cluster_scene(n_splats, seed=sseed, degree=3))
         fr.set_scene(splats, sh, deg)
         for d, cam in random_cameras(pkg, cams_per_scene, W, H, rng):
+            if time_budget_s is not None and time.perf_counter() - t0 > time_budget_s:
+                break
             seed = seed_base + 100_000 * k
-            a, f, ms_in = fr.accum(cam, p, seed, in_ens, features=True)
-            t, _, ms_t = fr.accum(cam, p, seed + 50_000, tgt_ens)
-            x = torch.zeros(P, 8, dtype=torch.bfloat16, device="cuda")
-            base = torch.zeros(P, 3, device="cuda")
-            dn.pack(a, f, x, base)
-            xs.append(x.view(H, W, 8))
-            bases.append(base.view(H, W, 3))
-            tgts.append(mean_rgb(t).view(H, W, 3).contiguous())
-            meta.append({"scene": [n_splats, sseed], "distance": d, "ms_input": ms_in, "ms_target": ms_t})
+            fr.r.reset_accum()
+            fr.feat.zero_()
+            fr.r.set_feature_accum(fr.feat)
+            fr.r.render_ensembles(cam, p, seed, in_ens)
+            fr.r.set_feature_accum(None)
+            dn._ck(L.gpsb_dn_pack(C.c_void_p(acc), dn._p(fr.feat), P, dn._p(xs[k]), dn._p(bases[k]),
+                                  C.c_void_p(stream)), "pack")
+            fr.r.reset_accum()
+            fr.r.render_ensembles(cam, p, seed + 50_000, tgt_ens)
+            dn._ck(L.gpsb_dn_mean_rgb(C.c_void_p(acc), P, dn._p(tgts[k]), C.c_void_p(stream)), "mean_rgb")
+            meta.append({"scene": [n_splats, sseed], "distance": d})
             k += 1
-    return torch.stack(xs), torch.stack(bases), torch.stack(tgts), meta
+            if log and k % 100 == 0:
+                torch.cuda.synchronize()
+                log(f"frames {k}/{N} after {time.perf_counter() - t0:.0f} s")
+        else:
+            continue
+        break
+    torch.cuda.synchronize()
+    fr.r.set_stream(None)
+    return xs[:k], bases[:k], tgts[:k], meta
 
 
 class CollapseGuard:
@@ -314,7 +341,18 @@ def main(argv=None):
     ap.add_argument("--crop", type=int, default=256)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--log-every", type=int, default=100)
+    ap.add_argument("--data-budget-s", type=float, default=None,
+                    help="stop rendering training frames after this many seconds (train on what was rendered)")
+    ap.add_argument("--protocol", default=None, choices=[None, "config4"],
+                    help="config4: 2,000 random orbit cameras over 8 seeded cluster scenes of 200k-1M Gaussians "
+                         "(250 each), 256-ensemble targets, evaluation on 64 held-out cameras of the same scenes "
+                         "against the plain 256-ensemble result")
     args = ap.parse_args(argv)
+    if args.protocol == "config4":
+        sc = ",".join(f"{int(round(200_000 + i * 800_000 / 7))}:{11 + i}" for i in range(8))
+        args.train_scenes, args.eval_scenes = sc, sc
+        args.train_cams, args.eval_cams, args.target_ens, args.ref_ens = 250, 8, 256, 256
     pkg = _pkg()
     from gps_pbvr_web_b200 import denoise as dn
     rng = np.random.default_rng(args.seed)
@@ -322,7 +360,8 @@ def main(argv=None):
     fr = FrameRenderer(pkg, args.width, args.height)
     t0 = time.perf_counter()
     x, base, target, meta = make_frames(pkg, fr, spec(args.train_scenes), args.train_cams, args.in_ens,
-                                        args.target_ens, rng, 1)
+                                        args.target_ens, rng, 1, time_budget_s=args.data_budget_s,
+                                        log=lambda m: print(m, file=sys.stderr, flush=True))
     t_data = time.perf_counter() - t0
     net = dn.Denoiser(seed=args.seed)
     if args.load:
@@ -330,12 +369,13 @@ def main(argv=None):
         hist, ms_step = [], 0.0
     else:
         guard = CollapseGuard()
-        hist, ms_step = train(net, x, base, target, args.steps, args.batch, args.crop, args.lr, rng, guard=guard)
+        hist, ms_step = train(net, x, base, target, args.steps, args.batch, args.crop, args.lr, rng, guard=guard,
+                              log_every=args.log_every)
         gate_limit = 1.5 * float(x[..., 5].float().mean(dim=(1, 2)).max())
     del x, base, target
     torch.cuda.empty_cache()
     rows = evaluate(pkg, net, fr, spec(args.eval_scenes), args.eval_cams, args.in_ens, args.ref_ens,
-                    [4, 8, 16, 32, 64, 128], rng, 7_000_000, gate_limit)
+                    [4, 8, 16, 32, 64, 128, 256], rng, 1_500_000_000, gate_limit)
     save_weights(net, args.weights, gate_limit)
     res = {"config": vars(args), "train_frames": len(meta), "data_seconds": t_data, "loss_history": hist,
            "guard_restores": [] if args.load else guard.restores,
