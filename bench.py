@@ -559,6 +559,79 @@ def run_stress(args, rank, world):
     return 0
 
 
+def run_case(args):
+    """Small single-kernel-family workloads for ncu captures (each a few launches of a case larger
+    than the 126 MB L2 but a few GB at most on the device); prints the device error word:
+      scan                 exclusive scan of 2^26 u32 counts, 3 times (k_scan_u32_staged)
+      sort                 stable radix sort of 2^24 (24-bit key, value) pairs, 8-bit digits, 3 times
+      denoise-train        two training steps of the denoiser on 2 x 256 x 256 crops
+      denoise-infer        two 1280 x 720 inferences of the denoiser (conv3 and the element-wise steps)
+      particles-near       PBVR Ext C3+R, 560k cluster scene, 1280 x 720, near view, 2 ensembles in one
+                           launch of k_particles, fast decisions on
+      particles-near-exact the same with the fast decisions off"""
+    import ctypes as C
+    import torch
+    pkg = load_package()
+    L = pkg.abi.lib()
+    case = args.case
+    g = torch.Generator(device="cuda").manual_seed(3)
+    err = 0
+    if case in ("scan", "sort"):
+        r = pkg.GpsRenderer(16, 16, 1)
+        if case == "scan":
+            n = 1 << 26
+            x = torch.randint(0, 16, (n,), dtype=torch.int32, device="cuda", generator=g)
+            y = torch.empty_like(x)
+            tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+            for _ in range(3):
+                assert L.gpsb_scan_u32(r.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), n,
+                                       C.c_void_p(tot.data_ptr())) == 0
+        else:
+            m = 1 << 24
+            keys = torch.randint(0, 1 << 24, (m,), dtype=torch.int32, device="cuda", generator=g)
+            vals = torch.arange(m, dtype=torch.int32, device="cuda")
+            kb, vb = torch.empty_like(keys), torch.empty_like(vals)
+            for _ in range(3):
+                ka, va = keys.clone(), vals.clone()
+                assert L.gpsb_sort_pairs(r.handle, C.c_void_p(ka.data_ptr()), C.c_void_p(va.data_ptr()),
+                                         C.c_void_p(kb.data_ptr()), C.c_void_p(vb.data_ptr()), m, 24) == 0
+                r.wait_idle()
+        r.wait_idle()
+        err = r.debug_error_word()
+        r.close()
+    elif case.startswith("denoise"):
+        from gps_pbvr_web_b200 import denoise as dn
+        net = dn.Denoiser()
+        dn.load_weights(net)
+        gc = torch.Generator().manual_seed(0)
+        if case == "denoise-train":
+            x0 = torch.zeros(2, 256, 256, 8)
+            x0[..., :6] = torch.rand(2, 256, 256, 6, generator=gc)
+            base = torch.rand(2, 256, 256, 3, generator=gc).cuda()
+            x0 = x0.to(torch.bfloat16).cuda()
+            for _ in range(2):
+                net.train_step(x0, base, base, lr=1e-4)
+        else:
+            x = torch.rand(1, H, W, 8, generator=gc).to(torch.bfloat16).cuda()
+            base = torch.zeros(1, H, W, 3, device="cuda")
+            for _ in range(2):
+                net.forward(x, base)
+        torch.cuda.synchronize()
+        err = net.error_word()
+    else:
+        splats, sh, deg = build_scene(pkg)
+        cam = cameras(pkg, ["near"])[0][1]
+        r = pkg.GpsRenderer(W, H, SIDE)
+        r.set_gaussians_sh(splats, sh, deg)
+        r.set_fast_decisions(0 if case == "particles-near-exact" else 1)
+        r.render_ensembles(cam, params(pkg), 1, 2)
+        torch.cuda.synchronize()
+        err = r.debug_error_word()
+        r.close()
+    print(case, "error word", err)
+    return 1 if err else 0
+
+
 def run_b200(args, rank, world):
     import torch
     pkg = load_package()
@@ -753,12 +826,17 @@ def main():
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64, help="splat fraction each host thread renders")
     ap.add_argument("--views", default="near,mid,far", help="subset of the views (small profiling cases)")
     ap.add_argument("--ensembles", type=int, default=ENS, help="ensembles per view (small profiling cases)")
+    ap.add_argument("--case", default=None,
+                    choices=["scan", "sort", "denoise-train", "denoise-infer", "particles-near", "particles-near-exact"],
+                    help="one small single-kernel-family workload for an ncu capture (no JSON line)")
     args = ap.parse_args()
     args.views = [v for v in args.views.split(",") if v]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.case:
+        return run_case(args)
     if args.config == "trajectory":
         return run_trajectory(args, rank, world)
     if args.config == "stress":

@@ -6,7 +6,7 @@ Sources (read from a checkout of the reference project):
   oracle (loaded by crates/gps-core/tests/cpp_crosscheck.rs:36-45);
   tests/fixtures/synthetic_sh1.ply -- a small binary SH-degree-1 3DGS file
   (generator tests/gen_synthetic_ply.py).
-Usage: python tests/golden/make_fixtures.py [reference_root]
+Usage: python tests/golden/make_fixtures.py <reference_root>
 """
 import hashlib
 import json
@@ -32,4 +32,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py <reference_root>")
+    main(sys.argv[1])

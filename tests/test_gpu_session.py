@@ -77,8 +77,13 @@ def test_half_resolution_mode():
     assert img.size == W * H * 4
     small = np.asarray(r.composite(p, w2, h2))
     assert small.size == w2 * h2 * 4
-    # the upsampled frame is the bilinear magnification of the half-size one: same mean brightness
-    assert abs(img.reshape(-1, 4)[:, :3].astype(np.float64).mean() - small.reshape(-1, 4)[:, :3].astype(np.float64).mean()) < 4.0
+    # the upsampling composite (gps_composite.wgsl:41-55) of the half-size accumulation at the odd
+    # output size, and the plain one at its own size, equal the O2 mirror byte for byte
+    import oracle as O
+    acc = r.read_accum()
+    for ow, oh, got in ((W, H, img), (w2, h2, small)):
+        want = O.o2_composite(acc, w2, h2, p.exposure, p.srgb_output, ow, oh)
+        assert np.array_equal(np.asarray(got).reshape(-1, 4), want), (ow, oh)
     r.close()
 
 
