@@ -521,6 +521,8 @@ def run_stress(args, rank, world):
                                    fov_y=0.9).to_camera(sw, sh_)) for name, d in VIEWS]
     per_view, stages = {}, {}
     P = sw * sh_
+    clocks = ClockSampler(0)
+    clocks.start()
     for name, cam in cams:
         r.reset_accum()
         r.render_ensembles(cam, p, 1, 1)  # warm-up
@@ -545,15 +547,25 @@ def run_stress(args, rank, world):
                 rows[sname] = {"ms": ms, "launches": launches, "alg_GBps": byts * launches / (ms / 1e3) / 1e9}
         stages[name] = {"stages": rows, "particles": st.particles, "points": st.points,
                         "subpixel_writes": st.subpixel_writes}
-    dnz = denoise_measure(pkg, r, stream, cams, p, per_view, ref_ens=args.stress_ref, w=sw, h=sh_,
-                          counts=(4, 16, 64, 256) if args.stress_ref > 256 else (4, 16, 64), big_ref=0)
+    clk = clocks.stop()
+    # reference ensembles per view (--stress-ref, overridden per view by --stress-ref-views)
+    refs = {name: args.stress_ref for name, _ in cams}
+    for item in filter(None, args.stress_ref_views.split(",")):
+        k, v = item.split(":")
+        refs[k] = int(v)
+    dnz = {"views": {}, "reference_ensembles": refs, "input_ensembles": 4}
+    for name, cam in cams:
+        one = denoise_measure(pkg, r, stream, [(name, cam)], p, per_view, ref_ens=refs[name], w=sw, h=sh_,
+                              counts=tuple(c for c in (4, 16, 64, 256) if c <= refs[name]), big_ref=0)
+        dnz["views"][name] = one["views"][name]
+        dnz["engine"] = one["engine"]
     line = {"metric": "stress: denoised 4-ensemble frames vs plain 64 / 256 ensembles", "unit": "dB, ms",
             "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": f"{n} synthetic Gaussians SH3, {sw}x{sh_} spp1, cap {args.stress_cap}, "
                                    "PBVR Extinction C3+R, near/mid/far orbit (2.5/7/20)",
                        "gaussians": n, "resolution": [sw, sh_], "cap": args.stress_cap,
-                       "reference_ensembles": args.stress_ref},
-            "ms_per_ensemble": per_view, "per_view": stages, "denoise": dnz}
+                       "reference_ensembles": refs},
+            "ms_per_ensemble": per_view, "per_view": stages, "clocks": clk, "denoise": dnz}
     print(json.dumps(line))
     r.close()
     return 0
@@ -823,6 +835,7 @@ def main():
     ap.add_argument("--stress-res", default="3840x2160")
     ap.add_argument("--stress-cap", type=int, default=65536)
     ap.add_argument("--stress-ref", type=int, default=256, help="ensembles of the stress reference")
+    ap.add_argument("--stress-ref-views", default="", help="per-view reference ensembles, e.g. near:64")
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64, help="splat fraction each host thread renders")
     ap.add_argument("--views", default="near,mid,far", help="subset of the views (small profiling cases)")
     ap.add_argument("--ensembles", type=int, default=ENS, help="ensembles per view (small profiling cases)")
