@@ -68,7 +68,7 @@ constexpr int kMaxPasses = 8;
 #endif
 constexpr int kRsLook = GPSB_SORT_LOOKAHEAD;  // predecessor tiles read per lookback round trip
 #ifndef GPSB_SORT_BALLOT_PEERS
-#define GPSB_SORT_BALLOT_PEERS 1  // 0 match.any, 1 ballots, 2 alternating per key
+#define GPSB_SORT_BALLOT_PEERS 1  // 0 match.any, 1 ballots, 2 alternating per key, 3 shared-memory OR
 #endif
 constexpr uint32_t kStAgg = 1u << 30, kStPre = 2u << 30, kStMask = (1u << 30) - 1u;
 
@@ -146,13 +146,25 @@ __global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesw
     uint32_t key[kRsIpt], rank[kRsIpt];
     const uint32_t lt = lanemask_lt();
     uint32_t* wc = s_wcnt[warp];
+    // peer masks through shared memory (variant 3): each warp's row of BINS words lives in the key
+    // staging area, which the ranking does not use yet (it is written after the block barrier that
+    // ends the ranking); rows start at zero and every group's lowest lane clears its digit's word
+    uint32_t* wm = s_key + warp * BINS;
+    if (GPSB_SORT_BALLOT_PEERS == 3) {
+        for (int k = lane; k < BINS; k += 32) wm[k] = 0u;
+        __syncwarp();
+    }
     // rank every key within its warp's sub-tile in input order (stable): the lanes holding one digit
     // find each other (peers: one ballot per digit bit, or match.any), every lane reads its digit's
     // running count of the warp, and the lowest lane of each group adds the group's size (the
     // groups hold distinct digits, so the warp's counter row needs no atomics)
     auto rank_key = [&](int q, uint32_t d, uint32_t live) {
         uint32_t peers;
-        if (GPSB_SORT_BALLOT_PEERS == 1 || (GPSB_SORT_BALLOT_PEERS == 2 && (q & 1))) {
+        if (GPSB_SORT_BALLOT_PEERS == 3) {
+            if ((live >> lane) & 1u) atomicOr(&wm[d], 1u << lane);
+            __syncwarp();
+            peers = wm[d] & live;
+        } else if (GPSB_SORT_BALLOT_PEERS == 1 || (GPSB_SORT_BALLOT_PEERS == 2 && (q & 1))) {
             peers = live;
 #pragma unroll
             for (int b = 0; b < BITS; ++b) {
@@ -166,7 +178,10 @@ __global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesw
         const uint32_t below = __popc(peers & lt);
         const uint32_t old = wc[d];
         __syncwarp();
-        if (below == 0u && ((live >> lane) & 1u)) wc[d] = old + (uint32_t)__popc(peers);
+        if (below == 0u && ((live >> lane) & 1u)) {
+            wc[d] = old + (uint32_t)__popc(peers);
+            if (GPSB_SORT_BALLOT_PEERS == 3) wm[d] = 0u;
+        }
         __syncwarp();  // orders this key's count update before the next key's reads
         rank[q] = old + below;
     };
