@@ -348,11 +348,13 @@ def main(argv=None):
                     help="config4: 2,000 random orbit cameras over 8 seeded cluster scenes of 200k-1M Gaussians "
                          "(250 each), 256-ensemble targets, evaluation on 64 held-out cameras of the same scenes "
                          "against the plain 256-ensemble result")
-    args = ap.parse_args(argv)
-    if args.protocol == "config4":
+    pre = argparse.ArgumentParser(add_help=False)
+    pre.add_argument("--protocol", default=None)
+    if pre.parse_known_args(argv)[0].protocol == "config4":  # its values become the defaults
         sc = ",".join(f"{int(round(200_000 + i * 800_000 / 7))}:{11 + i}" for i in range(8))
-        args.train_scenes, args.eval_scenes = sc, sc
-        args.train_cams, args.eval_cams, args.target_ens, args.ref_ens = 250, 8, 256, 256
+        ap.set_defaults(train_scenes=sc, eval_scenes=sc, train_cams=250, eval_cams=8, target_ens=256, ref_ens=256,
+                        steps=12000, log_every=200)
+    args = ap.parse_args(argv)
     pkg = _pkg()
     from gps_pbvr_web_b200 import denoise as dn
     rng = np.random.default_rng(args.seed)
