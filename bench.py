@@ -347,6 +347,13 @@ def micro_scan_sort(pkg, r, stream, peak):
         out[f"sort_pairs_{bits}bit"] = {"n": n, "ms": ms, "alg_bytes": alg, "GBps": alg / (ms / 1e3) / 1e9,
                                         "frac": alg / (ms / 1e3) / 1e9 / peak}
     r.set_tuning(sort_digit_bits=8)
+    # the sort by time: the fastest digit width against the fewest algorithmic bytes (8-bit digits:
+    # 4 B histogram read + 3 passes x 16 B = 52 B per pair), so extra passes do not count as bandwidth
+    best = min((k for k in out if k.startswith("sort_pairs_")), key=lambda k: out[k]["ms"])
+    alg8 = 52 * n
+    out["sort_pairs_by_time"] = {"n": n, "fastest": best, "ms": out[best]["ms"], "alg_bytes": alg8,
+                                 "GBps": alg8 / (out[best]["ms"] / 1e3) / 1e9,
+                                 "frac": alg8 / (out[best]["ms"] / 1e3) / 1e9 / peak}
     return out
 
 
