@@ -470,6 +470,8 @@ def run_trajectory(args, rank, world):
     out = torch.zeros(ncam * Wt * Ht * 4, device="cuda")
     E = args.ensembles
     rows = {}
+    clocks = ClockSampler(0)
+    clocks.start()
     with torch.cuda.stream(stream):
         for name, method in (("PBVR Extinction C3+R", pkg.Method.Extinction), ("ScreenOccupancy", pkg.Method.ScreenOccupancy)):
             p = pkg.RenderParams(spp_side=1, max_points_per_splat=CAP, method=method)
@@ -492,7 +494,8 @@ def run_trajectory(args, rank, world):
             rows[name] = {"ms_per_trajectory": ms, "gpu_launches_per_trajectory": (r.profile()["total_launches"] - l0) / args.steps, "ensembles_per_s": ncam * E / (ms / 1e3),
                           "ms_per_ensemble": ms / (ncam * E), "autotuned": best,
                           "sweep_ms": [[sh_, round(t, 3)] for sh_, t in sweep]}
-    line = {"metric": "ensembles/s (trajectory, captured CUDA graph)", "value": rows["PBVR Extinction C3+R"]["ensembles_per_s"],
+    clk = clocks.stop()
+    line = {"metric": "ensembles/s (trajectory, captured CUDA graph)", "clocks": clk, "value": rows["PBVR Extinction C3+R"]["ensembles_per_s"],
             "unit": "ensembles/s", "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "higher_is_better": True,
             "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": f"{n} synthetic Gaussians SH3, 1920x1080 spp1, cap {CAP}, 16-camera 360-degree orbit "
