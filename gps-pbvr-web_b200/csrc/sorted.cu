@@ -71,6 +71,9 @@ constexpr int kRsLook = GPSB_SORT_LOOKAHEAD;  // predecessor tiles read per look
 #define GPSB_SORT_BALLOT_PEERS 1  // 0 match.any, 1 ballots, 2 alternating per key, 3 shared-memory OR
 #endif
 constexpr uint32_t kStAgg = 1u << 30, kStPre = 2u << 30, kStMask = (1u << 30) - 1u;
+#ifndef GPSB_SORT_BULK_VALUES
+#define GPSB_SORT_BULK_VALUES 0  // 1: a full tile's values arrive by one cp.async.bulk (mbarrier), 0: 16-byte cp.async
+#endif
 
 template <int BITS>
 __global__ void __launch_bounds__(256) k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, int passes,
@@ -120,8 +123,16 @@ __global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesw
     uint16_t* s_src = reinterpret_cast<uint16_t*>(s_stage + 2 * kRsTile);
     __shared__ uint32_t s_wsum[kRsWarps];
     __shared__ uint32_t s_tile;
+    __shared__ __align__(8) uint64_t s_vbar;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+    if (tid == 0) {
+        s_tile = atomicAdd(tile_counter, 1u);
+        if (GPSB_SORT_BULK_VALUES) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_vbar))
+                         : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+    }
     for (int k = tid; k < kRsWarps * BINS; k += kRsThreads) (&s_wcnt[0][0])[k] = 0;
     __syncthreads();
     const uint32_t t = s_tile;
@@ -130,7 +141,18 @@ __global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesw
     const uint32_t base = tile0 + warp * 32 * kRsIpt;
     // the tile's values travel to shared memory asynchronously while the keys are ranked
     const bool vasync = (((uintptr_t)vin) & 15u) == 0;
-    if (!vasync) {
+    const bool vbulk = GPSB_SORT_BULK_VALUES && vasync && tile_n == (uint32_t)kRsTile;
+    if (vbulk) {
+        if (tid == 0) {
+            const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&s_vbar);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kRsTile * 4u)
+                         : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             (uint32_t)__cvta_generic_to_shared(s_vin)),
+                         "l"(vin + tile0), "r"(kRsTile * 4u), "r"(bar)
+                         : "memory");
+        }
+    } else if (!vasync) {
         for (uint32_t e = tid; e < tile_n; e += kRsThreads) s_vin[e] = vin[tile0 + e];
     } else {
         for (uint32_t c = tid; c < (uint32_t)kRsTile / 4u; c += kRsThreads) {
@@ -225,7 +247,22 @@ __global__ void __launch_bounds__(kRsThreads, RsShape<BITS>::min_blocks) k_onesw
     uint32_t wbase = 0;
     for (int w = 0; w < warp; ++w) wbase += s_wsum[w];
     if (tid < BINS) s_dstart[tid] = wbase + incl - cnt;
-    if (vasync) asm volatile("cp.async.wait_all;" ::: "memory");  // own copies done; the barrier shares them
+    if (vbulk) {
+        if (tid == 0) {  // the bulk copy has landed (bounded wait); the barrier below shares it
+            const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&s_vbar);
+            uint32_t ok = 0;
+            for (uint32_t i = 0; i < (1u << 24) && !ok; ++i)
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}"
+                    : "=r"(ok)
+                    : "r"(bar)
+                    : "memory");
+            if (!ok) atomicOr(err, ERR_SORT_LOOKBACK);
+        }
+    } else if (vasync) {
+        asm volatile("cp.async.wait_all;" ::: "memory");  // own copies done; the barrier shares them
+    }
     __syncthreads();
     // scatter into shared memory in digit order (stable); values follow through their input index
 #pragma unroll
