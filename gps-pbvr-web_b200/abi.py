@@ -174,12 +174,12 @@ SIGNATURES = {
     "gpsb_dn_conv3": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, P, P, ST, ST, ST, ST, P, P]),
     "gpsb_dn_conv_dw": (ST, [P, ST, P, ST, ST, ST, ST, ST, ST, ST, ST, P, P, P]),
     "gpsb_dn_flip": (ST, [P, ST, ST, ST, P, ST, ST, P]),
-    "gpsb_dn_relu_bwd": (ST, [P, ST, ST, P, ST, ST, ST, ST, P, ST, P]),
+    "gpsb_dn_relu_bwd": (ST, [P, ST, ST, P, ST, ST, ST, ST, ST, P, ST, P]),
     "gpsb_dn_up2": (ST, [P, ST, ST, ST, ST, ST, P, ST, ST, P]),
     "gpsb_dn_up2_bwd": (ST, [P, ST, ST, ST, ST, ST, ST, P, P]),
     "gpsb_dn_pool2": (ST, [P, ST, ST, ST, ST, ST, ST, P, P]),
     "gpsb_dn_pool2_bwd_add": (ST, [P, ST, ST, ST, ST, P, ST, ST, P]),
-    "gpsb_dn_bias_grad": (ST, [P, ST, ST, ST, P, P]),
+    "gpsb_dn_bias_grad": (ST, [P, ST, ST, ST, ST, P, P]),
     "gpsb_dn_l1": (ST, [P, P, P, ST, P, P, C.c_float, P]),
     "gpsb_dn_residual": (ST, [P, P, ST, P, P]),
     "gpsb_dn_adam": (ST, [P, P, P, P, ST, C.c_float, C.c_float, C.c_float, C.c_float, ST, P, P]),

@@ -1,6 +1,12 @@
-// Direct 3x3 convolution (stride 1, zero padding 1) of NHWC bf16 activations on the tcgen05 tensor
-// cores, with every operand staged by TMA: the denoiser's forward layers and the data gradients of
-// its backward pass (the same convolution with flipped weights).
+// Direct 3x3 convolution (stride 1, zero padding 1) of chunk-planar bf16 activations on the tcgen05
+// tensor cores, with every operand staged by TMA: the denoiser's forward layers and the data
+// gradients of its backward pass (the same convolution with flipped weights).
+//
+// Activation layout in HBM ("chunk-planar"): a bf16 tensor of C channels (C a multiple of 8) over B
+// images of H x W pixels is [B][C/8][H][W][8]: 8-channel chunk planes, each pixel's 8 channels of a
+// chunk in 16 contiguous bytes, a row of a plane contiguous. A channel slice [off, off + n) (both
+// multiples of 8) is a range of planes. fp32 outputs (the residual, the gradients) stay
+// pixel-major [B][H][W][ld].
 //
 //   Y[b][y][x][n] = act(bias[n] + sum_{dy,dx,ci} X[b][y+dy][x+dx][ci] W[n][(dy+1)*3 + (dx+1)][ci])
 //
@@ -8,9 +14,9 @@
 // channels. The K loop runs over groups of G input channels. One pipeline stage holds
 //   * the R + 2 input rows y0-1 .. y0+R of pixels x0-1 .. x0+128 of the group's channels, one
 //     plane per 8-channel chunk: [chunk][row][pixel][8 channels], 16 bytes per (row, pixel), loaded
-//     by one TMA box per chunk from a 5-D view (8 channels, chunk, W, H, B) of the activation
-//     tensor; pixels and rows outside the image read as zeros (TMA out-of-bounds fill), which is
-//     the convolution's padding;
+//     by ONE TMA box (8 channels, 130 pixels, R + 2 rows, G/8 chunks) from a 5-D view (8 channels,
+//     W, H, chunk, B) of the chunk-planar tensor, whose rows are 130 x 16 contiguous bytes; pixels
+//     and rows outside the image read as zeros (TMA out-of-bounds fill), which is the padding;
 //   * the group's weights in the canonical K-major layout of the MMA's B operand, one 1-D bulk copy
 //     of a block that gpsb_dn_conv3_weights arranged once: [tap][chunk][n][8 channels].
 // In the canonical K-major layout without swizzle a core matrix is 8 rows x 16 bytes, i.e. eight
@@ -59,13 +65,12 @@ struct Cfg {
     static constexpr int R = N <= 32 ? 8 : N <= 64 ? 4 : N <= 128 ? 2 : 1;
     static constexpr int G = N >= 192 ? 16 : 32;
     static constexpr int CH = G / 8;                                     // chunk planes per stage
-    static constexpr int BOX = (R + 2) * kHalo * 16;                     // bytes one TMA box writes
-    static constexpr int PLANE = round_up(BOX, 128);                     // plane stride in shared memory
-    static constexpr int IN = CH * PLANE;
+    static constexpr int PLANE = (R + 2) * kHalo * 16;                   // bytes of one chunk plane
+    static constexpr int IN = CH * PLANE;                                // the TMA box of one stage
     static constexpr int WB = 9 * CH * N * 16;                           // weight bytes of one group
     static constexpr int STAGE = round_up(IN + WB, 1024);
     static constexpr int S = N >= 192 ? 3 : 2;
-    static constexpr uint32_t TX = (uint32_t)(CH * BOX + WB);            // bytes landing per stage
+    static constexpr uint32_t TX = (uint32_t)(IN + WB);                  // bytes landing per stage
     static constexpr size_t SMEM = (size_t)S * STAGE + 1024;             // + alignment slack
     static_assert(R * N <= (int)kAccCols, "accumulator columns");
     static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N of one MMA");
@@ -127,7 +132,7 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
 struct Params {
     const bf16* wt;       // arranged weights: [group][tap][chunk][n][8]
     const float* bias;    // [cout] or null
-    void* out;            // [B][H][W][ldo] at channel offset ooff, bf16 or fp32
+    void* out;            // bf16: chunk-planar [B][ldo/8][H][W][8]; fp32: [B][H][W][ldo]; channels from ooff
     int ldo, ooff, out_f32, relu;
     int B, H, W, cout, groups;
     int segs, rowblocks, blocks;
@@ -199,8 +204,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
                     }
                     uint8_t* st = base + (size_t)stage * C::STAGE;
                     bar_expect(&s_full[stage], C::TX);
-                    for (int c = 0; c < C::CH; ++c)
-                        tma_load5(saddr(st + c * C::PLANE), &xmap, 0, g * C::CH + c, x0 - 1, y0 - 1, b, &s_full[stage]);
+                    tma_load5(saddr(st), &xmap, 0, x0 - 1, y0 - 1, g * C::CH, b, &s_full[stage]);
                     bulk_load(saddr(st + C::IN), p.wt + (size_t)g * (C::WB / 2), (uint32_t)C::WB, &s_full[stage]);
                     armed |= 1u << stage;
                     if (++stage == C::S) {
@@ -309,7 +313,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
             for (int r = 0; r < C::R; ++r) {
                 const int y = y0 + r;
                 const bool valid = x < p.W && y < p.H;
-                const size_t o = (((size_t)b * p.H + (valid ? y : 0)) * p.W + (valid ? x : 0)) * p.ldo + p.ooff;
+                const size_t pix = ((size_t)b * p.H + (valid ? y : 0)) * p.W + (valid ? x : 0);
+                const size_t plane = (size_t)p.H * p.W;  // pixels of one chunk plane
+                const size_t img = ((size_t)(valid ? y : 0)) * p.W + (valid ? x : 0);
 #pragma unroll 1
                 for (int c = 0; c < N; c += 16) {
                     float v[16];
@@ -321,28 +327,39 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
                         float s = v[k] + ((p.bias && n < p.cout) ? __ldg(&p.bias[n]) : 0.0f);
                         v[k] = p.relu ? fmaxf(s, 0.0f) : s;
                     }
-                    if (c + 16 <= p.cout && ((p.ldo | p.ooff) & 7) == 0) {
-                        if (p.out_f32) {
-                            float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(p.out) + o + c);
+                    if (p.out_f32) {
+                        float* o = reinterpret_cast<float*>(p.out) + pix * p.ldo + p.ooff + c;
+                        if (c + 16 <= p.cout && ((p.ldo | p.ooff) & 3) == 0) {
+                            float4* dst = reinterpret_cast<float4*>(o);
 #pragma unroll
                             for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
                         } else {
-                            uint32_t w[8];
 #pragma unroll
-                            for (int q = 0; q < 8; ++q) {
-                                __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
-                                w[q] = *reinterpret_cast<uint32_t*>(&h);
-                            }
-                            uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(p.out) + o + c);
-                            dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
-                            dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                            for (int k = 0; k < 16; ++k)
+                                if (c + k < p.cout) o[k] = v[k];
                         }
                     } else {
+                        // chunk-planar: output channels ooff + c .. + 15 are two 16-byte pixel slots of
+                        // planes (ooff + c) / 8 and + 1 (a warp stores 32 consecutive pixels of a plane)
+                        bf16* o = reinterpret_cast<bf16*>(p.out);
+                        const size_t base_b = (size_t)b * (p.ldo / 8);
 #pragma unroll
-                        for (int k = 0; k < 16; ++k) {
-                            if (c + k < p.cout) {
-                                if (p.out_f32) reinterpret_cast<float*>(p.out)[o + c + k] = v[k];
-                                else reinterpret_cast<bf16*>(p.out)[o + c + k] = __float2bfloat16_rn(v[k]);
+                        for (int h = 0; h < 2; ++h) {
+                            const int n0 = c + 8 * h;
+                            if (n0 >= p.cout) break;
+                            const size_t at = ((base_b + (size_t)((p.ooff + n0) >> 3)) * plane + img) * 8;
+                            if (n0 + 8 <= p.cout) {
+                                uint32_t w[4];
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    __nv_bfloat162 hh = __floats2bfloat162_rn(v[8 * h + 2 * q], v[8 * h + 2 * q + 1]);
+                                    w[q] = *reinterpret_cast<uint32_t*>(&hh);
+                                }
+                                *reinterpret_cast<uint4*>(o + at) = make_uint4(w[0], w[1], w[2], w[3]);
+                            } else {
+#pragma unroll
+                                for (int k = 0; k < 8; ++k)
+                                    if (n0 + k < p.cout) o[at + k] = __float2bfloat16_rn(v[8 * h + k]);
                             }
                         }
                     }
@@ -415,15 +432,17 @@ static cudaError_t launch(const bf16* x, int ldx, int xoff, int cin, const Param
     using Cf = Cfg<N>;
     auto enc = encoder();
     if (!enc) return cudaErrorNotSupported;
-    // 5-D view of the activations: (8 channels, chunk, W, H, B); channel chunks of [xoff, xoff + cin)
+    // 5-D view of the chunk-planar activations: (8 channels, W, H, chunk, B); the chunks of channels
+    // [xoff, xoff + cin) of a tensor of ldx channels
     CUtensorMap map;
-    const cuuint64_t dims[5] = {8, (cuuint64_t)((cin + 7) / 8), (cuuint64_t)prm.W, (cuuint64_t)prm.H, (cuuint64_t)prm.B};
-    const cuuint64_t strides[4] = {16, (cuuint64_t)ldx * 2, (cuuint64_t)prm.W * ldx * 2, (cuuint64_t)prm.H * prm.W * ldx * 2};
-    const cuuint32_t box[5] = {8, 1, (cuuint32_t)kHalo, (cuuint32_t)(Cf::R + 2), 1};
+    const cuuint64_t plane = (cuuint64_t)prm.W * prm.H * 16;  // bytes of one chunk plane
+    const cuuint64_t dims[5] = {8, (cuuint64_t)prm.W, (cuuint64_t)prm.H, (cuuint64_t)((cin + 7) / 8), (cuuint64_t)prm.B};
+    const cuuint64_t strides[4] = {16, (cuuint64_t)prm.W * 16, plane, plane * (cuuint64_t)(ldx / 8)};
+    const cuuint32_t box[5] = {8, (cuuint32_t)kHalo, (cuuint32_t)(Cf::R + 2), (cuuint32_t)Cf::CH, 1};
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)(x + xoff), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)(x + (size_t)(xoff / 8) * prm.W * prm.H * 8), dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     Params q = prm;
     q.segs = (prm.W + kSeg - 1) / kSeg;
@@ -466,14 +485,16 @@ int gpsb_dn_conv3_weights(const void* w, int cout, int cin, int kp, void* wt, vo
     return (int)cudaGetLastError();
 }
 
-// 3x3 convolution, stride 1, zero padding 1: NHWC bf16 input x (B, H, W, ldx) channels
-// [xoff, xoff + cin), arranged weights wt, output (B, H, W, ldo) channels [ooff, ooff + cout),
-// bf16 or fp32 (out_f32), optional bias and ReLU. ldx and xoff multiples of 8, x 16-byte aligned,
-// cout <= 192. Enqueues on `stream`; a device-side wait that gives up sets bit 32 of *err.
+// 3x3 convolution, stride 1, zero padding 1: chunk-planar bf16 input x of ldx channels (B, H, W),
+// channels [xoff, xoff + cin), arranged weights wt, output channels [ooff, ooff + cout) of a tensor
+// of ldo channels: bf16 chunk-planar (ooff a multiple of 8), or fp32 pixel-major (out_f32);
+// optional bias and ReLU. ldx, xoff multiples of 8, x 16-byte aligned, cout <= 192. Enqueues on
+// `stream`; a device-side wait that gives up sets bit 32 of *err.
 int gpsb_dn_conv3(const void* x, int ldx, int xoff, int cin, int B, int H, int W, const void* wt, int cout,
                   const float* bias, void* out, int ldo, int ooff, int out_f32, int relu, void* stream, uint32_t* err) {
     if (!x || !wt || !out || !err || ldx % 8 || xoff % 8 || cin < 1 || xoff + cin > ldx || cout < 1 || cout > 192 ||
-        B < 1 || H < 1 || W < 1 || ooff < 0 || ooff + cout > ldo || (reinterpret_cast<uintptr_t>(x) & 15u))
+        B < 1 || H < 1 || W < 1 || ooff < 0 || ooff + cout > ldo || (reinterpret_cast<uintptr_t>(x) & 15u) ||
+        (!out_f32 && (ldo % 8 || ooff % 8)))
         return (int)cudaErrorInvalidValue;
     Params prm{};
     prm.wt = (const bf16*)wt;

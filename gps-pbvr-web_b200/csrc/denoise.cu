@@ -1,8 +1,9 @@
-// Kernels of the learned denoiser: 3x3 convolutions (stride 1, zero padding 1) over NHWC bf16
-// activations as implicit GEMMs on the tcgen05 engine of umma.cuh, their weight gradients, and
-// the element-wise steps of the U-Net (ReLU backward, 2x2 average pooling, nearest upsampling,
-// L1 loss, Adam). Channel counts are padded to multiples of 8 so that every 16-byte chunk of an
-// activation row holds 8 channels of one pixel.
+// Kernels of the learned denoiser: 3x3 convolutions (stride 1, zero padding 1) as implicit GEMMs on
+// the tcgen05 engine of umma.cuh (the earlier engine, pixel-major NHWC in and out), the weight
+// gradients, and the element-wise steps of the U-Net (ReLU backward, 2x2 average pooling, nearest
+// upsampling, L1 loss, Adam). The network's bf16 activations are chunk-planar, [B][C/8][H][W][8]
+// (the layout conv3x3.cu reads with TMA); its fp32 buffers (gradients, residual) are pixel-major.
+// Channel counts are padded to multiples of 8; an 8-channel tensor is the same in both layouts.
 //
 //   forward   Y[p][n]  = act(bias[n] + sum_k Xcol[p][k] W[n][k]),  k = (ky*3 + kx)*Cin + ci
 //   data grad dX       = the forward convolution of dY with W'[ci][(2-ky)*3 + (2-kx)][co] = W[co][ky*3+kx][ci]
@@ -125,9 +126,9 @@ __device__ __forceinline__ void transpose8(const uint4* in, uint4* out) {
 }
 
 struct ConvDW {
-    const bf16* dy;     // [M][ldy] output gradient (bf16), cout channels at offset 0
+    const bf16* dy;     // output gradient, chunk-planar of ldy channels (bf16), cout channels at offset 0
     int ldy;
-    const bf16* x;      // layer input [M][ldx] at channel offset xoff, cin channels
+    const bf16* x;      // layer input, chunk-planar of ldx channels, cin channels at offset xoff
     int ldx, xoff, cin;
     int B, H, W;
     int cout, kp;
@@ -143,8 +144,10 @@ struct ConvDW {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int p = p0 + pg * 8 + q, c = m0 + cg * 8;
-            in[q] = (p < M && c < cout) ? __ldg(reinterpret_cast<const uint4*>(dy + (size_t)p * ldy + c))
-                                        : make_uint4(0u, 0u, 0u, 0u);
+            const int HW = H * W, b = p / HW, pix = p - b * HW;
+            in[q] = (p < M && c < cout)
+                        ? __ldg(reinterpret_cast<const uint4*>(dy + (((size_t)b * (ldy / 8) + c / 8) * HW + pix) * 8))
+                        : make_uint4(0u, 0u, 0u, 0u);
         }
         transpose8(in, out);
 #pragma unroll
@@ -167,7 +170,8 @@ struct ConvDW {
                     const int xq = p % W, yq = (p / W) % H, b = p / (W * H);
                     const int yy = yq + tap / 3 - 1, xx = xq + tap % 3 - 1;
                     if (yy >= 0 && yy < H && xx >= 0 && xx < W)
-                        v = __ldg(reinterpret_cast<const uint4*>(x + ((size_t)(b * H + yy) * W + xx) * ldx + xoff + ci));
+                        v = __ldg(reinterpret_cast<const uint4*>(
+                            x + ((((size_t)b * (ldx / 8) + (xoff + ci) / 8) * H + yy) * W + xx) * 8));
                 }
                 in[q] = v;
             }
@@ -221,27 +225,41 @@ __global__ void k_flip(const bf16* w, int cout, int cin, int kp, bf16* wf, int c
 // ---------------------------------------------------------------------------- element-wise steps
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 
-// out[m][c] = g[m][goff + c] * (y[m][yoff + c] > 0) for c < C (y null: no mask), 0 for C <= c < ldo
-__global__ void k_relu_bwd(const float* g, int ldg, int goff, const bf16* y, int ldy, int yoff, int M, int C, bf16* out,
-                           int ldo) {
-    const int i = gtid();
-    if (i >= M * ldo) return;
-    const int m = i / ldo, c = i - m * ldo;
+// out (chunk-planar, ldo channels, B images of HW pixels): channel c < C = g[pix][goff + c] (fp32
+// pixel-major) masked by y[pix][yoff + c] > 0 (chunk-planar, y null: no mask), 0 for C <= c < ldo
+__global__ void k_relu_bwd(const float* g, int ldg, int goff, const bf16* y, int ldy, int yoff, int B, int HW, int C,
+                           bf16* out, int ldo) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)B * HW * ldo) return;
+    const int e = (int)(i & 7);
+    long t = i >> 3;
+    const int pix = (int)(t % HW);
+    t /= HW;
+    const int ch = (int)(t % (ldo / 8)), b = (int)(t / (ldo / 8));
+    const int c = ch * 8 + e;
     float v = 0.0f;
     if (c < C) {
-        v = g[(size_t)m * ldg + goff + c];
-        if (y && !(__bfloat162float(y[(size_t)m * ldy + yoff + c]) > 0.0f)) v = 0.0f;
+        v = g[((size_t)b * HW + pix) * ldg + goff + c];
+        if (y && !(__bfloat162float(y[(((size_t)b * (ldy / 8) + (yoff + c) / 8) * HW + pix) * 8 + e]) > 0.0f)) v = 0.0f;
     }
     out[i] = __float2bfloat16_rn(v);
 }
 
-// nearest 2x upsampling of src (B, h, w, lds) channels [0, C) into dst (B, 2h, 2w, ldd) at doff
+// nearest 2x upsampling of src (chunk-planar, lds channels, B x h x w) channels [0, C) into dst
+// (chunk-planar, ldd channels, B x 2h x 2w) channels [doff, doff + C)
 __global__ void k_up2(const bf16* src, int lds, int B, int h, int w, int C, bf16* dst, int ldd, int doff) {
-    const int i = gtid();
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const int H = 2 * h, W = 2 * w;
-    if (i >= B * H * W * C) return;
-    const int c = i % C, px = i / C, X = px % W, Y = (px / W) % H, b = px / (W * H);
-    dst[(size_t)px * ldd + doff + c] = src[((size_t)(b * h + Y / 2) * w + X / 2) * lds + c];
+    if (i >= (long)B * H * W * C) return;
+    const int e = (int)(i & 7);
+    long t = i >> 3;
+    const int X = (int)(t % W);
+    t /= W;
+    const int Y = (int)(t % H);
+    t /= H;
+    const int ch = (int)(t % (C / 8)), b = (int)(t / (C / 8));
+    dst[((((size_t)b * (ldd / 8) + doff / 8 + ch) * H + Y) * W + X) * 8 + e] =
+        src[((((size_t)b * (lds / 8) + ch) * h + Y / 2) * w + X / 2) * 8 + e];
 }
 // out (B, h, w, C) = sum over each 2x2 block of g (B, 2h, 2w, ldg) channels [goff, goff + C)
 __global__ void k_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int C, float* out) {
@@ -254,16 +272,23 @@ __global__ void k_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w
     for (int d = 0; d < 4; ++d) s += g[((size_t)(b * 2 * h + 2 * y + (d >> 1)) * W + 2 * x + (d & 1)) * ldg + goff + c];
     out[i] = s;
 }
-// 2x2 average pooling of src (B, 2h, 2w, lds) channels [soff, soff + C) into dst (B, h, w, C)
+// 2x2 average pooling of src (chunk-planar, lds channels, B x 2h x 2w) channels [soff, soff + C) into
+// dst (chunk-planar, C channels, B x h x w)
 __global__ void k_pool2(const bf16* src, int lds, int soff, int B, int h, int w, int C, bf16* dst) {
-    const int i = gtid();
-    if (i >= B * h * w * C) return;
-    const int c = i % C, px = i / C, x = px % w, y = (px / w) % h, b = px / (w * h);
-    const int W = 2 * w;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)B * h * w * C) return;
+    const int e = (int)(i & 7);
+    long t = i >> 3;
+    const int x = (int)(t % w);
+    t /= w;
+    const int y = (int)(t % h);
+    t /= h;
+    const int ch = (int)(t % (C / 8)), b = (int)(t / (C / 8));
+    const int H = 2 * h, W = 2 * w;
+    const bf16* s0 = src + (((size_t)b * (lds / 8) + soff / 8 + ch) * H) * W * 8;
     float s = 0.0f;
 #pragma unroll
-    for (int d = 0; d < 4; ++d)
-        s += __bfloat162float(src[((size_t)(b * 2 * h + 2 * y + (d >> 1)) * W + 2 * x + (d & 1)) * lds + soff + c]);
+    for (int d = 0; d < 4; ++d) s += __bfloat162float(s0[((size_t)(2 * y + (d >> 1)) * W + 2 * x + (d & 1)) * 8 + e]);
     dst[i] = __float2bfloat16_rn(0.25f * s);
 }
 // acc (B, 2h, 2w, lda) channels [aoff, aoff + C) += g (B, h, w, C) / 4 spread over each 2x2 block
@@ -274,15 +299,17 @@ __global__ void k_pool2_bwd_add(const float* g, int B, int h, int w, int C, floa
     const int c = i % C, px = i / C, X = px % W, Y = (px / W) % H, b = px / (W * H);
     acc[(size_t)px * lda + aoff + c] += 0.25f * g[((size_t)(b * h + Y / 2) * w + X / 2) * C + c];
 }
-// db[c] += sum_m dz[m][c]: one block per 256-pixel chunk, shared partial sums, one atomic per channel
-__global__ void k_bias_grad(const bf16* dz, int ld, int M, int C, float* db) {
+// db[c] += sum over pixels of dz (chunk-planar, ld channels, B images of HW pixels) channel c: one
+// block per 256-pixel chunk of one image, shared partial sums, one atomic per channel
+__global__ void k_bias_grad(const bf16* dz, int ld, int B, int HW, int C, float* db) {
     __shared__ float s[256];
     for (int c = threadIdx.x; c < C; c += blockDim.x) s[c] = 0.0f;
     __syncthreads();
-    const int m0 = blockIdx.x * 256;
+    const int chunks = (HW + 255) / 256;
+    const int b = blockIdx.x / chunks, p0 = (blockIdx.x - b * chunks) * 256;
     for (int i = threadIdx.x; i < 256 * C; i += blockDim.x) {
-        const int m = m0 + i / C, c = i % C;
-        if (m < M) atomicAdd(&s[c], __bfloat162float(dz[(size_t)m * ld + c]));
+        const int c = i / 256, p = p0 + (i & 255);  // consecutive threads: consecutive pixels of a channel
+        if (p < HW) atomicAdd(&s[c], __bfloat162float(dz[(((size_t)b * (ld / 8) + c / 8) * HW + p) * 8 + (c & 7)]));
     }
     __syncthreads();
     for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&db[c], s[c]);
@@ -474,14 +501,15 @@ int gpsb_dn_flip(const void* w, int cout, int cin, int kp, void* wf, int coutp, 
 
 static inline int grid_of(long n) { return (int)((n + 255) / 256); }
 
-int gpsb_dn_relu_bwd(const float* g, int ldg, int goff, const void* y, int ldy, int yoff, int M, int C, void* out,
-                     int ldo, void* stream) {
-    if (C > ldo) return (int)cudaErrorInvalidValue;
-    k_relu_bwd<<<grid_of((long)M * ldo), 256, 0, (cudaStream_t)stream>>>(g, ldg, goff, (const bf16*)y, ldy, yoff, M, C,
-                                                                          (bf16*)out, ldo);
+int gpsb_dn_relu_bwd(const float* g, int ldg, int goff, const void* y, int ldy, int yoff, int B, int HW, int C,
+                     void* out, int ldo, void* stream) {
+    if (C > ldo || ldo % 8 || ldy % 8 || yoff % 8) return (int)cudaErrorInvalidValue;
+    k_relu_bwd<<<grid_of((long)B * HW * ldo), 256, 0, (cudaStream_t)stream>>>(g, ldg, goff, (const bf16*)y, ldy, yoff,
+                                                                               B, HW, C, (bf16*)out, ldo);
     return (int)cudaGetLastError();
 }
 int gpsb_dn_up2(const void* src, int lds, int B, int h, int w, int C, void* dst, int ldd, int doff, void* stream) {
+    if (C % 8 || lds % 8 || ldd % 8 || doff % 8) return (int)cudaErrorInvalidValue;
     k_up2<<<grid_of(4L * B * h * w * C), 256, 0, (cudaStream_t)stream>>>((const bf16*)src, lds, B, h, w, C, (bf16*)dst,
                                                                           ldd, doff);
     return (int)cudaGetLastError();
@@ -491,6 +519,7 @@ int gpsb_dn_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int 
     return (int)cudaGetLastError();
 }
 int gpsb_dn_pool2(const void* src, int lds, int soff, int B, int h, int w, int C, void* dst, void* stream) {
+    if (C % 8 || lds % 8 || soff % 8) return (int)cudaErrorInvalidValue;
     k_pool2<<<grid_of((long)B * h * w * C), 256, 0, (cudaStream_t)stream>>>((const bf16*)src, lds, soff, B, h, w, C,
                                                                              (bf16*)dst);
     return (int)cudaGetLastError();
@@ -499,9 +528,9 @@ int gpsb_dn_pool2_bwd_add(const float* g, int B, int h, int w, int C, float* acc
     k_pool2_bwd_add<<<grid_of(4L * B * h * w * C), 256, 0, (cudaStream_t)stream>>>(g, B, h, w, C, acc, lda, aoff);
     return (int)cudaGetLastError();
 }
-int gpsb_dn_bias_grad(const void* dz, int ld, int M, int C, float* db, void* stream) {
-    if (C > 256) return (int)cudaErrorInvalidValue;
-    k_bias_grad<<<(M + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const bf16*)dz, ld, M, C, db);
+int gpsb_dn_bias_grad(const void* dz, int ld, int B, int HW, int C, float* db, void* stream) {
+    if (C > 256 || ld % 8 || C > ld) return (int)cudaErrorInvalidValue;
+    k_bias_grad<<<B * ((HW + 255) / 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)dz, ld, B, HW, C, db);
     return (int)cudaGetLastError();
 }
 int gpsb_dn_l1(const float* base, const float* r, const float* target, int M, float* loss_sum, void* dr, float scale,

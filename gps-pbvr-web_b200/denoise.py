@@ -1,7 +1,9 @@
 """Learned denoiser of few-ensemble accumulations: a 3-level U-Net of 3x3 convolutions whose
 forward and backward passes run on the library's tcgen05 kernels (csrc/conv3x3.cu for the
 convolutions and data gradients, csrc/denoise.cu for the weight gradients and element-wise steps),
-with BF16 weights and activations and FP32 accumulation. PyTorch tensors only hold device memory here.
+with BF16 weights and activations and FP32 accumulation. bf16 activations are chunk-planar
+(B, C/8, H, W, 8) tensors, fp32 buffers pixel-major (B, H, W, C); the 8-channel input features
+are the same in both layouts. PyTorch tensors only hold device memory here.
 """
 import ctypes as C
 import os
@@ -49,20 +51,43 @@ def conv3_weights(w, cout, cin, wt=None):
     return wt
 
 
+def dims(t):
+    """(B, H, W, channels) of an activation tensor: chunk-planar bf16 (B, C/8, H, W, 8), or
+    pixel-major (B, H, W, C) (fp32 buffers, and 8-channel tensors, which are the same in both)."""
+    if t.dim() == 5:
+        B, C8, H, W, e = t.shape
+        assert e == 8
+        return B, H, W, 8 * C8
+    return tuple(t.shape)
+
+
+def to_planar(x):
+    """(B, H, W, C) pixel-major -> (B, C/8, H, W, 8) chunk-planar (contiguous copy)."""
+    B, H, W, C = x.shape
+    return x.reshape(B, H, W, C // 8, 8).permute(0, 3, 1, 2, 4).contiguous()
+
+
+def from_planar(x):
+    """(B, C/8, H, W, 8) chunk-planar -> (B, H, W, C) pixel-major."""
+    B, C8, H, W, _ = x.shape
+    return x.permute(0, 2, 3, 1, 4).reshape(B, H, W, 8 * C8)
+
+
 def conv3(x, cin, wt, cout, bias, out, *, xoff=0, ooff=0, relu=False, err):
-    """conv_fwd on the TMA-staged engine, with weights arranged by conv3_weights."""
+    """The 3x3 convolution on the TMA-staged engine (weights arranged by conv3_weights): x a
+    chunk-planar bf16 tensor, out chunk-planar bf16 or pixel-major fp32 (see dims)."""
     import torch
-    B, H, W, ldx = x.shape
-    ldo = out.shape[-1]
+    B, H, W, ldx = dims(x)
+    ldo = dims(out)[3]
     _ck(abi.lib().gpsb_dn_conv3(_p(x), ldx, xoff, cin, B, H, W, _p(wt), cout, _p(bias), _p(out), ldo, ooff,
                                 int(out.dtype == torch.float32), int(relu), _stream(), _p(err)), "conv3")
 
 
 def conv_dw(dy, x, cin, cout, dw, *, xoff=0, err):
     """dw (cout, kp) fp32 += weight gradient of the convolution of x channels [xoff, xoff + cin)
-    given the bf16 output gradient dy (B, H, W, ldy)."""
-    B, H, W, ldx = x.shape
-    _ck(abi.lib().gpsb_dn_conv_dw(_p(dy), dy.shape[-1], _p(x), ldx, xoff, cin, B, H, W, cout, dw.shape[1], _p(dw),
+    given the bf16 output gradient dy; dy and x chunk-planar (see dims)."""
+    B, H, W, ldx = dims(x)
+    _ck(abi.lib().gpsb_dn_conv_dw(_p(dy), dims(dy)[3], _p(x), ldx, xoff, cin, B, H, W, cout, dw.shape[1], _p(dw),
                                   _stream(), _p(err)), "conv_dw")
 
 
@@ -91,13 +116,9 @@ class Denoiser:
     to the few-ensemble mean colour. Master weights fp32 (Adam state beside them), compute copies
     bf16; every arithmetic step runs in the library's kernels."""
 
-    def __init__(self, seed=0, device="cuda", engine="tma"):
-        """engine: "tma" runs the convolutions and data gradients on conv3 (TMA-staged operands),
-        "cp.async" on the earlier implicit-im2col kernels (kept for comparison)."""
+    def __init__(self, seed=0, device="cuda"):
         import torch
-        if engine not in ("tma", "cp.async"):
-            raise ValueError("engine must be 'tma' or 'cp.async'")
-        self.engine = engine
+        self.engine = "tma"
         self.device = torch.device(device)
         g = torch.Generator().manual_seed(seed)
         self.p = {}
@@ -132,9 +153,8 @@ class Denoiser:
         for q in self.p.values():
             _ck(_L().gpsb_dn_to_bf16(_p(q["w"]), q["kp"], q["cout"], q["kp"], _p(q["wb"]), q["kp"], st), "to_bf16")
             flip(q["wb"], q["cout"], q["cin"], q["wf"], q["coutp"])
-            if self.engine == "tma":
-                q["wt"] = conv3_weights(q["wb"], q["cout"], q["cin"], q.get("wt"))
-                q["wft"] = conv3_weights(q["wf"], q["cin"], q["coutp"], q.get("wft"))
+            q["wt"] = conv3_weights(q["wb"], q["cout"], q["cin"], q.get("wt"))
+            q["wft"] = conv3_weights(q["wf"], q["cin"], q["coutp"], q.get("wft"))
 
     def state_dict(self):
         return {n: {"w": q["w"].cpu(), "b": q["b"].cpu()} for n, q in self.p.items()}
@@ -166,7 +186,9 @@ class Denoiser:
         d, bf, f32 = self.device, torch.bfloat16, torch.float32
         h2, w2, h4, w4 = H // 2, W // 2, H // 4, W // 4
 
-        def t(h, w, c, dt):
+        def t(h, w, c, dt):  # bf16 activations chunk-planar, fp32 buffers pixel-major
+            if dt == bf:
+                return torch.zeros(B, c // 8, h, w, 8, dtype=dt, device=d)
             return torch.zeros(B, h, w, c, dtype=dt, device=d)
         b = {
             "a1": t(H, W, 32, bf), "cat1": t(H, W, 96, bf), "p1": t(h2, w2, 32, bf), "a2": t(h2, w2, 64, bf),
@@ -185,7 +207,9 @@ class Denoiser:
         d, bf, f32 = self.device, torch.bfloat16, torch.float32
         h2, w2, h4, w4 = H // 2, W // 2, H // 4, W // 4
 
-        def t(h, w, c, dt):
+        def t(h, w, c, dt):  # bf16 gradients chunk-planar, fp32 ones pixel-major
+            if dt == bf:
+                return torch.zeros(B, c // 8, h, w, 8, dtype=dt, device=d)
             return torch.zeros(B, h, w, c, dtype=dt, device=d)
         g = {
             "dr": t(H, W, 8, bf), "dz1": t(H, W, 32, bf), "dz2": t(h2, w2, 64, bf), "dz4": t(h4, w4, 128, bf),
@@ -198,10 +222,7 @@ class Denoiser:
     # ------------------------------------------------------------------ forward
     def _conv(self, name, x, out, *, xoff=0, ooff=0, relu=True):
         q = self.p[name]
-        if self.engine == "tma":
-            conv3(x, q["cin"], q["wt"], q["cout"], q["b"], out, xoff=xoff, ooff=ooff, relu=relu, err=self.err)
-        else:
-            conv_fwd(x, q["cin"], q["wb"], q["cout"], q["b"], out, xoff=xoff, ooff=ooff, relu=relu, err=self.err)
+        conv3(x, q["cin"], q["wt"], q["cout"], q["b"], out, xoff=xoff, ooff=ooff, relu=relu, err=self.err)
 
     def forward(self, x0, base):
         """x0 (B, H, W, 8) bf16 features, base (B, H, W, 3) fp32 mean colour -> prediction (B, H, W, 3)."""
@@ -231,18 +252,15 @@ class Denoiser:
     def _back(self, name, dz, x, gx, *, xoff=0, data_grad=True):
         """weight, bias and (optionally) input gradients of layer `name` from its bf16 output gradient dz"""
         q = self.p[name]
-        B, H, W, _ = dz.shape
+        B, H, W, ld = dims(dz)
         conv_dw(dz, x, q["cin"], q["cout"], q["gw"], xoff=xoff, err=self.err)
-        _ck(_L().gpsb_dn_bias_grad(_p(dz), dz.shape[-1], B * H * W, q["cout"], _p(q["gb"]), _stream()), "bias_grad")
+        _ck(_L().gpsb_dn_bias_grad(_p(dz), ld, B, H * W, q["cout"], _p(q["gb"]), _stream()), "bias_grad")
         if data_grad:
-            if self.engine == "tma":
-                conv3(dz, q["coutp"], q["wft"], q["cin"], None, gx, err=self.err)
-            else:
-                conv_fwd(dz, q["coutp"], q["wf"], q["cin"], None, gx, err=self.err)
+            conv3(dz, q["coutp"], q["wft"], q["cin"], None, gx, err=self.err)
 
     def _relu_bwd(self, g, ldg, goff, y, ldy, yoff, C, out):
-        B, H, W, ldo = out.shape
-        _ck(_L().gpsb_dn_relu_bwd(_p(g), ldg, goff, _p(y), ldy, yoff, B * H * W, C, _p(out), ldo, _stream()),
+        B, H, W, ldo = dims(out)
+        _ck(_L().gpsb_dn_relu_bwd(_p(g), ldg, goff, _p(y), ldy, yoff, B, H * W, C, _p(out), ldo, _stream()),
             "relu_bwd")
 
     def backward(self, x0, base, target):

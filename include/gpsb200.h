@@ -419,44 +419,54 @@ gpsb_status gpsb_session_read_state(const gpsb_session* s, gpsb_session_state* o
 /* ------------------------------------------------------------------- denoiser kernels
  * The learned denoiser of few-ensemble frames (the "denoised batch vs plain" comparison). The
  * reference has no denoiser, so none of these has a counterpart in it. All pointers are device
- * memory; activations are NHWC (pixel-major, channels innermost) bf16 with channel counts padded
- * to multiples of 8; weights are (cout, kp) bf16 rows, k = (ky*3 + kx)*cin + ci, kp a multiple of
- * 64 >= 9*cin. Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream); the
+ * memory. The network's bf16 activations are chunk-planar, [B][C/8][H][W][8] (8-channel planes,
+ * one pixel's 8 channels of a plane in 16 contiguous bytes), channel counts padded to multiples
+ * of 8, a channel slice [off, off + n) being the planes off/8 ..; its fp32 buffers (gradients,
+ * residual) are pixel-major [B][H][W][C]. An 8-channel tensor is the same in both layouts.
+ * gpsb_dn_conv_fwd (the earlier engine) reads and writes pixel-major tensors. Weights are
+ * (cout, kp) bf16 rows, k = (ky*3 + kx)*cin + ci, kp a multiple of 64 >= 9*cin. Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream); the
  * return value is a cudaError_t code (0 = launched). `err` (a device word) receives a non-zero
  * bit when a bounded device-side wait gives up. */
 /* y[p][ooff+n] = act(bias[n] + sum_k xcol[p][k] w[n][k]): 3x3 convolution, stride 1, zero padding
- * 1, on the tcgen05 tensor cores; out is bf16, or fp32 when out_f32; relu != 0 applies ReLU. */
+ * 1, on the tcgen05 tensor cores (implicit im2col through 16-byte copies); pixel-major x and out;
+ * out is bf16, or fp32 when out_f32; relu != 0 applies ReLU. */
 int gpsb_dn_conv_fwd(const void* x, int ldx, int xoff, int cin, int B, int H, int W, const void* w, int cout,
                      int kp, const float* bias, void* out, int ldo, int ooff, int out_f32, int relu,
                      void* stream, uint32_t* err);
-/* The same convolution with TMA-staged operands (persistent, warp-specialised CTAs: the input rows
- * of an R-row x 128-pixel block are staged once as 8-channel planes and the nine taps are shifted
- * shared-memory descriptors over them; two tensor-memory accumulators overlap the epilogue with the
- * next block's MMAs). Weights come pre-arranged by gpsb_dn_conv3_weights into a buffer of
- * gpsb_dn_conv3_weight_bytes(cout, cin) bytes. x 16-byte aligned, ldx and xoff multiples of 8,
- * cout <= 192; a bounded device-side wait that gives up sets bit 32 of *err (err required). */
+/* The same convolution on chunk-planar activations with TMA-staged operands (persistent,
+ * warp-specialised CTAs: one TMA box stages the input rows of an R-row x 128-pixel block as
+ * 8-channel planes and the nine taps are shifted shared-memory descriptors over them; two
+ * tensor-memory accumulators overlap the epilogue with the next block's MMAs). x: chunk-planar of
+ * ldx channels; out: chunk-planar bf16 of ldo channels, or pixel-major fp32 (out_f32). Weights come
+ * pre-arranged by gpsb_dn_conv3_weights into a buffer of gpsb_dn_conv3_weight_bytes(cout, cin)
+ * bytes. x 16-byte aligned, ldx and xoff multiples of 8 (and ldo, ooff for bf16 out), cout <= 192;
+ * a bounded device-side wait that gives up sets bit 32 of *err (err required). */
 unsigned long long gpsb_dn_conv3_weight_bytes(int cout, int cin);
 int gpsb_dn_conv3_weights(const void* w, int cout, int cin, int kp, void* wt, void* stream);
 int gpsb_dn_conv3(const void* x, int ldx, int xoff, int cin, int B, int H, int W, const void* wt, int cout,
                   const float* bias, void* out, int ldo, int ooff, int out_f32, int relu, void* stream,
                   uint32_t* err);
-/* dw[co][k] += sum_p dy[p][co] * xcol[p][k] (fp32, caller-zeroed): the weight gradient. */
+/* dw[co][k] += sum_p dy[p][co] * xcol[p][k] (fp32, caller-zeroed): the weight gradient; dy and x
+ * chunk-planar. */
 int gpsb_dn_conv_dw(const void* dy, int ldy, const void* x, int ldx, int xoff, int cin, int B, int H, int W,
                     int cout, int kp, float* dw, void* stream, uint32_t* err);
 /* wf[ci][(8 - t)*coutp + co] = w[co][t*cin + ci]: weights of the data gradient (a forward conv). */
 int gpsb_dn_flip(const void* w, int cout, int cin, int kp, void* wf, int coutp, int kp2, void* stream);
-/* out[m][c] = g[m][goff+c] * (y[m][yoff+c] > 0) as bf16 (y NULL: no mask), zero for C <= c < ldo. */
-int gpsb_dn_relu_bwd(const float* g, int ldg, int goff, const void* y, int ldy, int yoff, int M, int C, void* out,
-                     int ldo, void* stream);
-/* nearest 2x upsampling into a channel slice, and its gradient (sum over 2x2 blocks). */
+/* out (chunk-planar bf16, ldo channels, B images of HW pixels) channel c = g[pix][goff+c] (fp32
+ * pixel-major) * (y channel yoff+c > 0) (chunk-planar; y NULL: no mask) for c < C, zero above. */
+int gpsb_dn_relu_bwd(const float* g, int ldg, int goff, const void* y, int ldy, int yoff, int B, int HW, int C,
+                     void* out, int ldo, void* stream);
+/* nearest 2x upsampling into a channel slice (chunk-planar), and its gradient (fp32 pixel-major,
+ * sum over 2x2 blocks). */
 int gpsb_dn_up2(const void* src, int lds, int B, int h, int w, int C, void* dst, int ldd, int doff, void* stream);
 int gpsb_dn_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int C, float* out, void* stream);
-/* 2x2 average pooling of a channel slice, and its gradient added into a channel slice. */
+/* 2x2 average pooling of a channel slice (chunk-planar), and its gradient added into a channel
+ * slice (fp32 pixel-major). */
 int gpsb_dn_pool2(const void* src, int lds, int soff, int B, int h, int w, int C, void* dst, void* stream);
 int gpsb_dn_pool2_bwd_add(const float* g, int B, int h, int w, int C, float* acc, int lda, int aoff,
                           void* stream);
-/* db[c] += sum over M pixels of dz[m][c] (bf16 dz, C <= 256). */
-int gpsb_dn_bias_grad(const void* dz, int ld, int M, int C, float* db, void* stream);
+/* db[c] += sum over the B x HW pixels of dz channel c (chunk-planar bf16 of ld channels, C <= 256). */
+int gpsb_dn_bias_grad(const void* dz, int ld, int B, int HW, int C, float* db, void* stream);
 /* L1 loss of base + r against target (M x 3 fp32): loss_sum += sum |d|; dr (M x 8 bf16) = scale*sign(d). */
 int gpsb_dn_l1(const float* base, const float* r, const float* target, int M, float* loss_sum, void* dr,
                float scale, void* stream);

@@ -81,7 +81,7 @@ def test_conv_weight_and_data_gradient(cin, cout):
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     # weight gradient
     dw = torch.zeros(cout, wb.shape[1], device="cuda")
-    dn.conv_dw(dyb.cuda(), xb, cin, cout, dw, err=err)
+    dn.conv_dw(dn.to_planar(dyb).cuda(), dn.to_planar(xb), cin, cout, dw, err=err)  # chunk-planar operands
     torch.cuda.synchronize()
     ref_w = G.conv2d_weight(x_t, w_t.shape, dy_t, padding=1)  # (cout, cin, 3, 3)
     got_w = dw.cpu()[:, :9 * cin].reshape(cout, 3, 3, cin).permute(0, 3, 1, 2)

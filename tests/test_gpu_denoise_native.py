@@ -36,7 +36,7 @@ def setup():
 
 def test_native_forward_equals_python_sequencing():
     dn = _dn()
-    net = dn.Denoiser(engine="tma")
+    net = dn.Denoiser()
     dn.load_weights(net)
     nat = dn.NativeDenoiser()
     g = torch.Generator().manual_seed(2)
@@ -53,7 +53,7 @@ def test_native_forward_equals_python_sequencing():
 def test_render_denoised_through_the_c_abi(setup):
     r, cam, p = setup
     dn = _dn()
-    net = dn.Denoiser(engine="tma")
+    net = dn.Denoiser()
     gate = dn.load_weights(net)
     rgb_py, used_py, chk_py = dn.render_denoised(r, net, cam, p, 1000, ensembles=4, gate_limit=gate)
     nat = dn.NativeDenoiser()
@@ -69,7 +69,7 @@ def test_render_denoised_falls_back_when_the_check_fails(setup):
     (the 4 rendered ones plus the next seeds) is returned, in the Python and the C sequencing."""
     r, cam, p = setup
     dn = _dn()
-    net = dn.Denoiser(engine="tma")
+    net = dn.Denoiser()
     dn.load_weights(net)
     nat = dn.NativeDenoiser()
     rgb, used, chk = nat.render(r, cam, p, 2000, ensembles=4, gate_limit=1e-9, fallback_ensembles=16)
