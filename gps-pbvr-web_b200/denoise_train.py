@@ -376,6 +376,8 @@ def main(argv=None):
         gate_limit = 1.5 * float(x[..., 5].float().mean(dim=(1, 2)).max())
     del x, base, target
     torch.cuda.empty_cache()
+    if not args.load:  # the weights are kept even if the evaluation does not finish
+        save_weights(net, args.weights, gate_limit)
     rows = evaluate(pkg, net, fr, spec(args.eval_scenes), args.eval_cams, args.in_ens, args.ref_ens,
                     [4, 8, 16, 32, 64, 128, 256], rng, 1_500_000_000, gate_limit)
     save_weights(net, args.weights, gate_limit)
