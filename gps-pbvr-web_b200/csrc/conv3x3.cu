@@ -13,10 +13,12 @@
 // Work unit ("block"): R output rows x one 128-pixel row segment of one image, all N output
 // channels. The K loop runs over groups of G input channels. One pipeline stage holds
 //   * the R + 2 input rows y0-1 .. y0+R of pixels x0-1 .. x0+128 of the group's channels, one
-//     plane per 8-channel chunk: [chunk][row][pixel][8 channels], 16 bytes per (row, pixel), loaded
-//     by ONE TMA box (8 channels, 130 pixels, R + 2 rows, G/8 chunks) from a 5-D view (8 channels,
-//     W, H, chunk, B) of the chunk-planar tensor, whose rows are 130 x 16 contiguous bytes; pixels
-//     and rows outside the image read as zeros (TMA out-of-bounds fill), which is the padding;
+//     plane per 8-channel chunk: [chunk][row][pixel][8 channels], 16 bytes per (row, pixel), rows
+//     kRow = 2176 bytes apart (130 pixels used, padded so every row starts 128-byte aligned). TMA
+//     splits a box into one request per innermost box row, so the chunk-planar tensor is viewed
+//     as 8-byte elements (2 per pixel): each staged row is one 2048-byte box (128 pixels) and one
+//     32-byte box (the last 2 halo pixels), issued by the lanes of the producer warp; pixels and
+//     rows outside the image read as zeros (TMA out-of-bounds fill), which is the padding;
 //   * the group's weights in the canonical K-major layout of the MMA's B operand, one 1-D bulk copy
 //     of a block that gpsb_dn_conv3_weights arranged once: [tap][chunk][n][8 channels].
 // In the canonical K-major layout without swizzle a core matrix is 8 rows x 16 bytes, i.e. eight
@@ -51,6 +53,7 @@ using bf16 = __nv_bfloat16;
 
 constexpr int kSeg = 128;             // output pixels of a row segment (the MMA's M)
 constexpr int kHalo = kSeg + 2;       // staged input pixels per row
+constexpr int kRow = 2176;            // bytes between staged rows: 130 x 16 used, 128-byte aligned
 constexpr int kThreads = 192;         // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr uint32_t kAccCols = 256;    // tensor-memory columns of one accumulator (two are allocated)
 constexpr uint32_t kSpin = 1u << 24;  // polls of a bounded wait
@@ -65,12 +68,12 @@ struct Cfg {
     static constexpr int R = N <= 32 ? 8 : N <= 64 ? 4 : N <= 128 ? 2 : 1;
     static constexpr int G = N >= 192 ? 16 : 32;
     static constexpr int CH = G / 8;                                     // chunk planes per stage
-    static constexpr int PLANE = (R + 2) * kHalo * 16;                   // bytes of one chunk plane
-    static constexpr int IN = CH * PLANE;                                // the TMA box of one stage
+    static constexpr int PLANE = (R + 2) * kRow;                         // bytes of one chunk plane
+    static constexpr int IN = CH * PLANE;                                // staged input rows of a stage
     static constexpr int WB = 9 * CH * N * 16;                           // weight bytes of one group
     static constexpr int STAGE = round_up(IN + WB, 1024);
     static constexpr int S = N >= 192 ? 3 : 2;
-    static constexpr uint32_t TX = (uint32_t)(IN + WB);                  // bytes landing per stage
+    static constexpr uint32_t TX = (uint32_t)(CH * (R + 2) * kHalo * 16 + WB);  // bytes landing per stage
     static constexpr size_t SMEM = (size_t)S * STAGE + 1024;             // + alignment slack
     static_assert(R * N <= (int)kAccCols, "accumulator columns");
     static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N of one MMA");
@@ -114,12 +117,12 @@ __device__ __forceinline__ void bar_arrive(uint64_t* b) {
 __device__ __forceinline__ void bar_expect(uint64_t* b, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
 }
-// one 5-D TMA tile load into shared memory, completion counted on the mbarrier
-__device__ __forceinline__ void tma_load5(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+// one 4-D TMA tile load into shared memory, completion counted on the mbarrier
+__device__ __forceinline__ void tma_load4(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
                                           uint64_t* bar) {
     asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
-        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(saddr(bar))
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(saddr(bar))
         : "memory");
 }
 // one contiguous bulk copy global -> shared (16-byte aligned, size a multiple of 16)
@@ -140,7 +143,8 @@ struct Params {
 };
 
 template <int N>
-__global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ CUtensorMap xmap, const Params p) {
+__global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ CUtensorMap xmap,
+                                                     const __grid_constant__ CUtensorMap xtail, const Params p) {
     using C = Cfg<N>;
     extern __shared__ __align__(1024) uint8_t s_raw[];
     __shared__ __align__(8) uint64_t s_full[C::S], s_empty[C::S], s_acc_full[2], s_acc_empty[2], s_drain;
@@ -189,43 +193,60 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
 
     if (warp == 0) {
         // ------------------------------------------------------------------ TMA producer
+        // lane 0 waits for a free stage and arms its barrier; the 32 lanes then issue the stage's
+        // (R + 2) x CH row pairs (a 2048-byte box and a 32-byte box each); lane 0 adds the weights
         uint32_t armed = 0;  // stages armed at least once (for the abort drain)
         if (lane == 0) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
-            int stage = 0;
-            uint32_t phase = 0;
-            for (int blk = blockIdx.x; blk < p.blocks && !s_abort; blk += gridDim.x) {
-                int b, y0, x0;
-                decode(blk, b, y0, x0);
-                for (int g = 0; g < p.groups; ++g) {
-                    if (!bar_wait(&s_empty[stage], phase ^ 1u, &s_abort)) {
-                        fail();
-                        break;
-                    }
-                    uint8_t* st = base + (size_t)stage * C::STAGE;
-                    bar_expect(&s_full[stage], C::TX);
-                    tma_load5(saddr(st), &xmap, 0, x0 - 1, y0 - 1, g * C::CH, b, &s_full[stage]);
-                    bulk_load(saddr(st + C::IN), p.wt + (size_t)g * (C::WB / 2), (uint32_t)C::WB, &s_full[stage]);
-                    armed |= 1u << stage;
-                    if (++stage == C::S) {
-                        stage = 0;
-                        phase ^= 1u;
-                    }
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xtail)) : "memory");
+        }
+        int stage = 0;
+        uint32_t phase = 0;
+        bool stop = false;
+        for (int blk = blockIdx.x; blk < p.blocks && !stop; blk += gridDim.x) {
+            int b, y0, x0;
+            decode(blk, b, y0, x0);
+            for (int g = 0; g < p.groups; ++g) {
+                int ok = 1;
+                if (lane == 0) {
+                    ok = (!s_abort && bar_wait(&s_empty[stage], phase ^ 1u, &s_abort)) ? 1 : 0;
+                    if (!ok) fail();
+                    else bar_expect(&s_full[stage], C::TX);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    stop = true;
+                    break;
+                }
+                uint8_t* st = base + (size_t)stage * C::STAGE;
+                for (int t = lane; t < C::CH * (C::R + 2); t += 32) {
+                    const int c = t / (C::R + 2), rr = t - c * (C::R + 2);
+                    const uint32_t row = saddr(st + c * C::PLANE + rr * kRow);
+                    const int y = y0 - 1 + rr, ch = g * C::CH + c;
+                    tma_load4(row, &xmap, 2 * (x0 - 1), y, ch, b, &s_full[stage]);
+                    tma_load4(row + 2048u, &xtail, 2 * (x0 + kSeg - 1), y, ch, b, &s_full[stage]);
+                }
+                if (lane == 0) bulk_load(saddr(st + C::IN), p.wt + (size_t)g * (C::WB / 2), (uint32_t)C::WB, &s_full[stage]);
+                armed |= 1u << stage;
+                if (++stage == C::S) {
+                    stage = 0;
+                    phase ^= 1u;
                 }
             }
-            if (s_abort) {
-                // let this CTA's copies land before the CTA can exit: every stage's last armed phase
-                // completes by its transaction count alone
-                int st2 = stage;
-                uint32_t ph2 = phase;
-                for (int k = 0; k < C::S; ++k) {
-                    if (--st2 < 0) {
-                        st2 = C::S - 1;
-                        ph2 ^= 1u;
-                    }
-                    if (armed & (1u << st2)) {
-                        for (uint32_t i = 0; i < kSpin && !bar_test(&s_full[st2], ph2); ++i) {
-                        }
+        }
+        __syncwarp();
+        if (lane == 0 && s_abort) {
+            // let this CTA's copies land before the CTA can exit: every stage's last armed phase
+            // completes by its transaction count alone
+            int st2 = stage;
+            uint32_t ph2 = phase;
+            for (int k = 0; k < C::S; ++k) {
+                if (--st2 < 0) {
+                    st2 = C::S - 1;
+                    ph2 ^= 1u;
+                }
+                if (armed & (1u << st2)) {
+                    for (uint32_t i = 0; i < kSpin && !bar_test(&s_full[st2], ph2); ++i) {
                     }
                 }
             }
@@ -261,7 +282,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
                             const int dy = t / 3, dx = t % 3;  // input row r + dy, pixel offset dx (staged from -1)
 #pragma unroll
                             for (int j = 0; j < C::CH / 2; ++j) {
-                                const uint32_t aa = st + (uint32_t)(2 * j) * C::PLANE + (uint32_t)((r + dy) * kHalo + dx) * 16u;
+                                const uint32_t aa = st + (uint32_t)(2 * j) * C::PLANE + (uint32_t)((r + dy) * kRow + dx * 16);
                                 const uint32_t bb = wb + (uint32_t)((t * C::CH + 2 * j) * N) * 16u;
                                 umma::mma_bf16(acc + (uint32_t)(r * N), desc(aa, C::PLANE, 128), desc(bb, N * 16, 128),
                                                idesc, g > 0 || t > 0 || j > 0);
@@ -432,17 +453,23 @@ static cudaError_t launch(const bf16* x, int ldx, int xoff, int cin, const Param
     using Cf = Cfg<N>;
     auto enc = encoder();
     if (!enc) return cudaErrorNotSupported;
-    // 5-D view of the chunk-planar activations: (8 channels, W, H, chunk, B); the chunks of channels
-    // [xoff, xoff + cin) of a tensor of ldx channels
-    CUtensorMap map;
+    // 4-D view of the chunk-planar activations as 8-byte elements: (2 W, H, chunk, B), the chunks of
+    // channels [xoff, xoff + cin) of a tensor of ldx channels; boxes of one staged row: 256
+    // elements (128 pixels) and 4 elements (2 pixels)
+    CUtensorMap map, tail;
     const cuuint64_t plane = (cuuint64_t)prm.W * prm.H * 16;  // bytes of one chunk plane
-    const cuuint64_t dims[5] = {8, (cuuint64_t)prm.W, (cuuint64_t)prm.H, (cuuint64_t)((cin + 7) / 8), (cuuint64_t)prm.B};
-    const cuuint64_t strides[4] = {16, (cuuint64_t)prm.W * 16, plane, plane * (cuuint64_t)(ldx / 8)};
-    const cuuint32_t box[5] = {8, (cuuint32_t)kHalo, (cuuint32_t)(Cf::R + 2), (cuuint32_t)Cf::CH, 1};
-    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)(x + (size_t)(xoff / 8) * prm.W * prm.H * 8), dims,
-                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const cuuint64_t dims[4] = {(cuuint64_t)prm.W * 2, (cuuint64_t)prm.H, (cuuint64_t)((cin + 7) / 8), (cuuint64_t)prm.B};
+    const cuuint64_t strides[3] = {(cuuint64_t)prm.W * 16, plane, plane * (cuuint64_t)(ldx / 8)};
+    const cuuint32_t box[4] = {2 * kSeg, 1, 1, 1}, box_tail[4] = {4, 1, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    void* gaddr = (void*)(x + (size_t)(xoff / 8) * prm.W * prm.H * 8);
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, gaddr, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+        r = enc(&tail, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, gaddr, dims, strides, box_tail, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     Params q = prm;
     q.segs = (prm.W + kSeg - 1) / kSeg;
@@ -456,7 +483,7 @@ static cudaError_t launch(const bf16* x, int ldx, int xoff, int cin, const Param
     if (e != cudaSuccess) return e;
     const int grid = q.blocks < sms ? q.blocks : sms;
     if (grid <= 0) return cudaSuccess;
-    k_conv3<N><<<grid, kThreads, Cf::SMEM, st>>>(map, q);
+    k_conv3<N><<<grid, kThreads, Cf::SMEM, st>>>(map, tail, q);
     return cudaGetLastError();
 }
 
