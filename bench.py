@@ -555,8 +555,11 @@ def run_stress(args, rank, world):
                 byts = algorithmic_bytes_per_launch(sname, st.subpixel_writes / launches, st.list_entries / launches,
                                                     4, n, P)
                 rows[sname] = {"ms": ms, "launches": launches, "alg_GBps": byts * launches / (ms / 1e3) / 1e9}
+        # an ensemble whose particle total passes 2^32 - 1 is skipped (the reference's u32 rule,
+        # gps_splat.wgsl:635-663); candidates is the particle demand before the per-splat cap
         stages[name] = {"stages": rows, "particles": st.particles, "points": st.points,
-                        "subpixel_writes": st.subpixel_writes}
+                        "subpixel_writes": st.subpixel_writes, "skipped_ensembles": st.skipped_ensembles,
+                        "ensembles": st.ensembles, "candidates_before_cap": st.candidates}
     clk = clocks.stop()
     # reference ensembles per view (--stress-ref, overridden per view by --stress-ref-views)
     refs = {name: args.stress_ref for name, _ in cams}

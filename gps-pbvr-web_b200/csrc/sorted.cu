@@ -4,7 +4,8 @@
 //                   GPS demand probe, plus the screen-tile rectangle of the splat.
 //   radix_sort_pairs  stable LSD onesweep sort (replaces gps_sort.wgsl): one histogram pass for
 //                   all digits, then one kernel per digit that ranks keys within each warp by
-//                   peer groups (one ballot per digit bit), resolves tile offsets by a decoupled
+//                   peer groups (each lane ORs its bit into its digit's word of a per-warp row in
+//                   shared memory and reads the word back), resolves tile offsets by a decoupled
 //                   lookback per digit and scatters. Digit width 4, 6 or 8 bits.
 //   tile binning    (tile id, sorted rank) entries, stably sorted by tile, give every screen tile its
 //                   splats in depth order.
@@ -68,11 +69,13 @@ constexpr int kMaxPasses = 8;
 #endif
 constexpr int kRsLook = GPSB_SORT_LOOKAHEAD;  // predecessor tiles read per lookback round trip
 #ifndef GPSB_SORT_BALLOT_PEERS
-#define GPSB_SORT_BALLOT_PEERS 1  // 0 match.any, 1 ballots, 2 alternating per key, 3 shared-memory OR
+// 0 match.any, 1 ballots, 2 alternating per key, 3 shared-memory OR (2^26 pairs, 8-bit digits:
+// ballots 1.421 ms, shared OR 1.368, with the bulk value copy 1.330; A/B on one B200)
+#define GPSB_SORT_BALLOT_PEERS 3
 #endif
 constexpr uint32_t kStAgg = 1u << 30, kStPre = 2u << 30, kStMask = (1u << 30) - 1u;
 #ifndef GPSB_SORT_BULK_VALUES
-#define GPSB_SORT_BULK_VALUES 0  // 1: a full tile's values arrive by one cp.async.bulk (mbarrier), 0: 16-byte cp.async
+#define GPSB_SORT_BULK_VALUES 1  // 1: a full tile's values arrive by one cp.async.bulk (mbarrier), 0: 16-byte cp.async
 #endif
 
 template <int BITS>
