@@ -274,18 +274,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t st = saddr(base + (size_t)stage * C::STAGE);
-                    const uint32_t wb = st + C::IN;
+                    // one descriptor per operand and stage; every MMA adds a compile-time byte
+                    // offset / 16 to its 14-bit start-address field (shared addresses stay below
+                    // 256 KB, so the field never carries into the offsets above it)
+                    const uint64_t a0 = desc(st, C::PLANE, 128), b0 = desc(st + C::IN, N * 16, 128);
 #pragma unroll 1
                     for (int r = 0; r < C::R; ++r) {
+                        const uint64_t ar = a0 + (uint64_t)(r * (kRow / 16));
+                        const uint32_t d = acc + (uint32_t)(r * N);
 #pragma unroll
                         for (int t = 0; t < 9; ++t) {
+                            constexpr int kRow16 = kRow / 16;
                             const int dy = t / 3, dx = t % 3;  // input row r + dy, pixel offset dx (staged from -1)
 #pragma unroll
                             for (int j = 0; j < C::CH / 2; ++j) {
-                                const uint32_t aa = st + (uint32_t)(2 * j) * C::PLANE + (uint32_t)((r + dy) * kRow + dx * 16);
-                                const uint32_t bb = wb + (uint32_t)((t * C::CH + 2 * j) * N) * 16u;
-                                umma::mma_bf16(acc + (uint32_t)(r * N), desc(aa, C::PLANE, 128), desc(bb, N * 16, 128),
-                                               idesc, g > 0 || t > 0 || j > 0);
+                                const uint64_t ad = ar + (uint64_t)(2 * j * (C::PLANE / 16) + dy * kRow16 + dx);
+                                const uint64_t bd = b0 + (uint64_t)((t * C::CH + 2 * j) * N);
+                                umma::mma_bf16(d, ad, bd, idesc, g > 0 || t > 0 || j > 0);
                             }
                         }
                     }
