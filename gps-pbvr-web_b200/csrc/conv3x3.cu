@@ -27,11 +27,12 @@
 // size, stride byte offset = 128 bytes): the nine taps are nine descriptors over the same staged
 // rows, so each input byte crosses from L2 once per block instead of nine times.
 //
-// Roles (persistent CTAs, one per SM, 192 threads): warp 0 issues the TMA copies, one thread of
+// Roles (persistent CTAs, one per SM, 320 threads): warp 0 issues the TMA copies, one thread of
 // warp 1 issues the MMAs (M = 128 pixels, N, K = 16) into one of two tensor-memory accumulators of
-// R x N fp32 columns, warps 2-5 read the other accumulator back (tcgen05.ld, warp w reads lanes
-// 32 (w % 4) ..) and apply bias, ReLU and the bf16 / fp32 store, so the epilogue of block i
-// overlaps the MMAs of block i + 1. Stages and accumulators hand over through mbarriers (TMA
+// R x N fp32 columns, warps 2-9 read the other accumulator back (tcgen05.ld, warp w reads lanes
+// 32 (w % 4) .., two warps per lane quarter taking alternate 32-column pairs, two loads per wait)
+// and apply bias (staged once per CTA in shared memory), ReLU and the bf16 / fp32 store, so the
+// epilogue of block i overlaps the MMAs of block i + 1. Stages and accumulators hand over through mbarriers (TMA
 // transaction counts, tcgen05.commit, epilogue arrivals). Every wait is bounded: a wait that gives
 // up sets bit CONV3_ERR_TIMEOUT in the caller's error word and raises an abort flag that ends every
 // role; the CTA then waits (bounded) for its own TMA copies and MMAs before it frees its tensor
@@ -54,7 +55,8 @@ using bf16 = __nv_bfloat16;
 constexpr int kSeg = 128;             // output pixels of a row segment (the MMA's M)
 constexpr int kHalo = kSeg + 2;       // staged input pixels per row
 constexpr int kRow = 2176;            // bytes between staged rows: 130 x 16 used, 128-byte aligned
-constexpr int kThreads = 192;         // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kThreads = 320;         // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int kEpiWarps = 8;          // two per tensor-memory lane quarter
 constexpr uint32_t kAccCols = 256;    // tensor-memory columns of one accumulator (two are allocated)
 constexpr uint32_t kSpin = 1u << 24;  // polls of a bounded wait
 constexpr uint32_t CONV3_ERR_TIMEOUT = 32u;
@@ -142,6 +144,60 @@ struct Params {
     uint32_t* err;
 };
 
+// Bias, ReLU and the store of output channels c .. c + 15 of pixel (b, y, x): v the 16 accumulator
+// columns, bias the 16 staged bias values (16-byte aligned).
+__device__ __forceinline__ void store16(const Params& p, float* v, const float* bias, int b, int y, int x, int c) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 bq = reinterpret_cast<const float4*>(bias)[q];
+        v[4 * q] += bq.x;
+        v[4 * q + 1] += bq.y;
+        v[4 * q + 2] += bq.z;
+        v[4 * q + 3] += bq.w;
+    }
+    if (p.relu) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k], 0.0f);
+    }
+    const size_t pix = ((size_t)b * p.H + y) * p.W + x;
+    if (p.out_f32) {
+        float* o = reinterpret_cast<float*>(p.out) + pix * p.ldo + p.ooff + c;
+        if (c + 16 <= p.cout && ((p.ldo | p.ooff) & 3) == 0) {
+            float4* dst = reinterpret_cast<float4*>(o);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if (c + k < p.cout) o[k] = v[k];
+        }
+        return;
+    }
+    // chunk-planar: output channels ooff + c .. + 15 are two 16-byte pixel slots of planes
+    // (ooff + c) / 8 and + 1 (a warp stores 32 consecutive pixels of a plane)
+    bf16* o = reinterpret_cast<bf16*>(p.out);
+    const size_t plane = (size_t)p.H * p.W, img = (size_t)y * p.W + x, base_b = (size_t)b * (p.ldo / 8);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int n0 = c + 8 * h;
+        if (n0 >= p.cout) break;
+        const size_t at = ((base_b + (size_t)((p.ooff + n0) >> 3)) * plane + img) * 8;
+        if (n0 + 8 <= p.cout) {
+            uint32_t w[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                __nv_bfloat162 hh = __floats2bfloat162_rn(v[8 * h + 2 * q], v[8 * h + 2 * q + 1]);
+                w[q] = *reinterpret_cast<uint32_t*>(&hh);
+            }
+            *reinterpret_cast<uint4*>(o + at) = make_uint4(w[0], w[1], w[2], w[3]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (n0 + k < p.cout) o[at + k] = __float2bfloat16_rn(v[8 * h + k]);
+        }
+    }
+}
+
 template <int N>
 __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ CUtensorMap xmap,
                                                      const __grid_constant__ CUtensorMap xtail, const Params p) {
@@ -150,9 +206,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
     __shared__ __align__(8) uint64_t s_full[C::S], s_empty[C::S], s_acc_full[2], s_acc_empty[2], s_drain;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
+    __shared__ __align__(16) float s_bias[N];  // bias of the N accumulator columns (0 past cout)
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_raw) + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
+    for (int n = tid; n < N; n += kThreads) s_bias[n] = (p.bias && n < p.cout) ? p.bias[n] : 0.0f;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&s_tmem)),
                      "r"(2u * kAccCols)
@@ -166,7 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
         }
         for (int a = 0; a < 2; ++a) {
             bar_init(&s_acc_full[a], 1);
-            bar_init(&s_acc_empty[a], 4);
+            bar_init(&s_acc_empty[a], kEpiWarps);
         }
         bar_init(&s_drain, 1);
         s_abort = 0;
@@ -320,8 +378,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
         }
         __syncwarp();
     } else {
-        // ------------------------------------------------------------------ epilogue (warps 2-5)
-        const int quad = warp & 3;  // tensor-memory lanes 32 quad ..
+        // ------------------------------------------------------------------ epilogue (warps 2-9)
+        // the accumulator of a block is R x N columns = R N / 16 units of 16 columns (unit u: output
+        // row u / (N / 16), channels 16 (u % (N / 16)) ..); warp w reads tensor-memory lanes
+        // 32 (w % 4) .. (its 32 pixels) and takes every other pair of units, so two warps share each
+        // lane quarter; a pair is two loads and one wait
+        constexpr int kPairs = C::R * N / 32;
+        static_assert(C::R * N % 32 == 0, "whole pairs of 16-column units");
+        const int quad = warp & 3, half = (warp - 2) >> 2;
         const int px = quad * 32 + lane;
         int a = 0;
         uint32_t aphase = 0;
@@ -336,59 +400,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
             const int x = x0 + px;
             const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)a * kAccCols;
 #pragma unroll 1
-            for (int r = 0; r < C::R; ++r) {
-                const int y = y0 + r;
-                const bool valid = x < p.W && y < p.H;
-                const size_t pix = ((size_t)b * p.H + (valid ? y : 0)) * p.W + (valid ? x : 0);
-                const size_t plane = (size_t)p.H * p.W;  // pixels of one chunk plane
-                const size_t img = ((size_t)(valid ? y : 0)) * p.W + (valid ? x : 0);
-#pragma unroll 1
-                for (int c = 0; c < N; c += 16) {
-                    float v[16];
-                    umma::tmem_ld16(lane_base + (uint32_t)(r * N + c), v);  // every lane: .sync.aligned
-                    if (!valid) continue;
+            for (int pr = half; pr < kPairs; pr += 2) {
+                float v[32];
+                umma::tmem_ld16_issue(lane_base + (uint32_t)(pr * 32), v);
+                umma::tmem_ld16_issue(lane_base + (uint32_t)(pr * 32 + 16), v + 16);
+                umma::tmem_ld_wait(v);
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const int n = c + k;
-                        float s = v[k] + ((p.bias && n < p.cout) ? __ldg(&p.bias[n]) : 0.0f);
-                        v[k] = p.relu ? fmaxf(s, 0.0f) : s;
-                    }
-                    if (p.out_f32) {
-                        float* o = reinterpret_cast<float*>(p.out) + pix * p.ldo + p.ooff + c;
-                        if (c + 16 <= p.cout && ((p.ldo | p.ooff) & 3) == 0) {
-                            float4* dst = reinterpret_cast<float4*>(o);
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-                        } else {
-#pragma unroll
-                            for (int k = 0; k < 16; ++k)
-                                if (c + k < p.cout) o[k] = v[k];
-                        }
-                    } else {
-                        // chunk-planar: output channels ooff + c .. + 15 are two 16-byte pixel slots of
-                        // planes (ooff + c) / 8 and + 1 (a warp stores 32 consecutive pixels of a plane)
-                        bf16* o = reinterpret_cast<bf16*>(p.out);
-                        const size_t base_b = (size_t)b * (p.ldo / 8);
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int n0 = c + 8 * h;
-                            if (n0 >= p.cout) break;
-                            const size_t at = ((base_b + (size_t)((p.ooff + n0) >> 3)) * plane + img) * 8;
-                            if (n0 + 8 <= p.cout) {
-                                uint32_t w[4];
-#pragma unroll
-                                for (int q = 0; q < 4; ++q) {
-                                    __nv_bfloat162 hh = __floats2bfloat162_rn(v[8 * h + 2 * q], v[8 * h + 2 * q + 1]);
-                                    w[q] = *reinterpret_cast<uint32_t*>(&hh);
-                                }
-                                *reinterpret_cast<uint4*>(o + at) = make_uint4(w[0], w[1], w[2], w[3]);
-                            } else {
-#pragma unroll
-                                for (int k = 0; k < 8; ++k)
-                                    if (n0 + k < p.cout) o[at + k] = __float2bfloat16_rn(v[8 * h + k]);
-                            }
-                        }
-                    }
+                for (int h = 0; h < 2; ++h) {
+                    const int u = 2 * pr + h, y = y0 + u / (N / 16), c = (u % (N / 16)) * 16;
+                    if (x < p.W && y < p.H) store16(p, v + 16 * h, s_bias + c, b, y, x, c);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -93,6 +93,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// The same load without the wait: several loads can be in flight before one tmem_ld_wait(), after
+// which (and not before) v holds the columns.
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, float* v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
+          "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
+        : "r"(taddr)
+        : "memory");
+}
+// Waits for this thread's tensor-memory loads; every register of v is passed through an empty asm
+// after the wait, so the compiler can schedule no use of a loaded value before it.
+template <int n>
+__device__ __forceinline__ void tmem_ld_wait(float (&v)[n]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < n; ++i) asm volatile("" : "+f"(v[i]));
+}
+
 template <int BN>
 __host__ __device__ constexpr uint32_t tmem_cols() {
     return BN <= 32 ? 32u : BN <= 64 ? 64u : BN <= 128 ? 128u : 256u;
