@@ -27,12 +27,19 @@
 // size, stride byte offset = 128 bytes): the nine taps are nine descriptors over the same staged
 // rows, so each input byte crosses from L2 once per block instead of nine times.
 //
-// Roles (persistent CTAs, one per SM, 320 threads): warp 0 issues the TMA copies, one thread of
+// A tensor-core MMA of M = 128, K = 16 costs about 50 clocks however small N is (it reads the 4 KB
+// A tile from shared memory each time), so for N <= 64 the three vertical taps share one MMA of
+// width 3 N: staged row sr feeds output rows sr - 2 .. sr, whose accumulators are consecutive
+// column blocks, through B = the taps dy = 2, 1, 0 stacked (weights arranged [dx][chunk][dy][n][8]);
+// that is (R + 2) x 3 MMAs per chunk pair instead of R x 9.
+//
+// Roles (persistent CTAs, one per SM, 576 threads): warp 0 issues the TMA copies, one thread of
 // warp 1 issues the MMAs (M = 128 pixels, N, K = 16) into one of two tensor-memory accumulators of
-// R x N fp32 columns, warps 2-9 read the other accumulator back (tcgen05.ld, warp w reads lanes
-// 32 (w % 4) .., two warps per lane quarter taking alternate 32-column pairs, two loads per wait)
-// and apply bias (staged once per CTA in shared memory), ReLU and the bf16 / fp32 store, so the
-// epilogue of block i overlaps the MMAs of block i + 1. Stages and accumulators hand over through mbarriers (TMA
+// R x N fp32 columns, warps 2-17 read the other accumulator back (tcgen05.ld, warp w reads lanes
+// 32 (w % 4) .., four warps per lane quarter taking every fourth 32-column pair, two loads per
+// wait) and apply bias (staged once per CTA in shared memory), ReLU and the bf16 /
+// fp32 store, so the epilogue of block i overlaps the MMAs of block i + 1. Stages and accumulators
+// hand over through mbarriers (TMA
 // transaction counts, tcgen05.commit, epilogue arrivals). Every wait is bounded: a wait that gives
 // up sets bit CONV3_ERR_TIMEOUT in the caller's error word and raises an abort flag that ends every
 // role; the CTA then waits (bounded) for its own TMA copies and MMAs before it frees its tensor
@@ -55,21 +62,23 @@ using bf16 = __nv_bfloat16;
 constexpr int kSeg = 128;             // output pixels of a row segment (the MMA's M)
 constexpr int kHalo = kSeg + 2;       // staged input pixels per row
 constexpr int kRow = 2176;            // bytes between staged rows: 130 x 16 used, 128-byte aligned
-constexpr int kThreads = 320;         // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
-constexpr int kEpiWarps = 8;          // two per tensor-memory lane quarter
+constexpr int kThreads = 576;         // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
+constexpr int kEpiWarps = 16;         // four per tensor-memory lane quarter
 constexpr uint32_t kAccCols = 256;    // tensor-memory columns of one accumulator (two are allocated)
 constexpr uint32_t kSpin = 1u << 24;  // polls of a bounded wait
 constexpr uint32_t CONV3_ERR_TIMEOUT = 32u;
 
 __host__ __device__ constexpr int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-// Per output-channel width N: R rows per block (R x N <= 256 accumulator columns), G channels per
-// stage, S stages, and the byte layout of a stage.
-template <int N>
+// Per output-channel width N and chunk planes per stage CHS: R rows per block (R x N <= 256
+// accumulator columns), G = 8 CHS channels per stage, S stages, the byte layout of a stage, and
+// whether the three vertical taps share one MMA (STACK: 3 N <= 256, see the MMA issuer).
+template <int N, int CHS>
 struct Cfg {
     static constexpr int R = N <= 32 ? 8 : N <= 64 ? 4 : N <= 128 ? 2 : 1;
-    static constexpr int G = N >= 192 ? 16 : 32;
-    static constexpr int CH = G / 8;                                     // chunk planes per stage
+    static constexpr int CH = CHS;                                       // chunk planes per stage
+    static constexpr int G = 8 * CH;
+    static constexpr bool STACK = 3 * N <= 256;
     static constexpr int PLANE = (R + 2) * kRow;                         // bytes of one chunk plane
     static constexpr int IN = CH * PLANE;                                // staged input rows of a stage
     static constexpr int WB = 9 * CH * N * 16;                           // weight bytes of one group
@@ -80,7 +89,11 @@ struct Cfg {
     static_assert(R * N <= (int)kAccCols, "accumulator columns");
     static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N of one MMA");
     static_assert(SMEM <= 232448, "shared memory per CTA");
+    static_assert(CH % 2 == 0, "an MMA reads two chunk planes (K = 16)");
 };
+
+// chunk planes per stage of the instance serving N outputs and cin inputs
+__host__ __device__ constexpr int chs_of(int N, int cin) { return (N >= 192 || cin <= 16) ? 2 : 4; }
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -198,10 +211,10 @@ __device__ __forceinline__ void store16(const Params& p, float* v, const float* 
     }
 }
 
-template <int N>
+template <int N, int CHS>
 __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ CUtensorMap xmap,
                                                      const __grid_constant__ CUtensorMap xtail, const Params p) {
-    using C = Cfg<N>;
+    using C = Cfg<N, CHS>;
     extern __shared__ __align__(1024) uint8_t s_raw[];
     __shared__ __align__(8) uint64_t s_full[C::S], s_empty[C::S], s_acc_full[2], s_acc_empty[2], s_drain;
     __shared__ uint32_t s_tmem;
@@ -335,20 +348,57 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
                     // one descriptor per operand and stage; every MMA adds a compile-time byte
                     // offset / 16 to its 14-bit start-address field (shared addresses stay below
                     // 256 KB, so the field never carries into the offsets above it)
-                    const uint64_t a0 = desc(st, C::PLANE, 128), b0 = desc(st + C::IN, N * 16, 128);
+                    if constexpr (C::STACK) {
+                        // Staged row sr (image row y0 - 1 + sr) feeds output rows sr - 2, sr - 1, sr
+                        // through the vertical taps dy = 2, 1, 0. The group's B operand of (dx, chunk)
+                        // holds the three taps' N x 8 blocks stacked in that order, so one MMA of
+                        // width (hi - lo + 1) N writes the accumulators of output rows lo .. hi, which
+                        // lie in consecutive N-column blocks. Output row sr is first written by staged
+                        // row sr (tap dy = 0) at dx = 0, first chunk pair, group 0: that block is split
+                        // off and written without accumulation.
+                        const uint64_t a0 = desc(st, C::PLANE, 128), b0 = desc(st + C::IN, 3 * N * 16, 128);
+                        constexpr uint32_t id1 = umma::idesc_bf16(N), id2 = umma::idesc_bf16(2 * N),
+                                           id3 = umma::idesc_bf16(3 * N);
 #pragma unroll 1
-                    for (int r = 0; r < C::R; ++r) {
-                        const uint64_t ar = a0 + (uint64_t)(r * (kRow / 16));
-                        const uint32_t d = acc + (uint32_t)(r * N);
+                        for (int sr = 0; sr < C::R + 2; ++sr) {
+                            const int lo = sr > 2 ? sr - 2 : 0, hi = sr < C::R - 1 ? sr : C::R - 1;
+                            const int rows = hi - lo + 1;
+                            const uint32_t idn = rows == 3 ? id3 : rows == 2 ? id2 : id1;
+                            const uint32_t dlo = acc + (uint32_t)(lo * N);
+                            const int boff = (lo - sr + 2) * N;  // stacked row of output row lo's tap
+                            const uint64_t ar = a0 + (uint64_t)(sr * (kRow / 16));
+                            const bool fresh = g == 0 && hi == sr;
 #pragma unroll
-                        for (int t = 0; t < 9; ++t) {
-                            constexpr int kRow16 = kRow / 16;
-                            const int dy = t / 3, dx = t % 3;  // input row r + dy, pixel offset dx (staged from -1)
+                            for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
-                            for (int j = 0; j < C::CH / 2; ++j) {
-                                const uint64_t ad = ar + (uint64_t)(2 * j * (C::PLANE / 16) + dy * kRow16 + dx);
-                                const uint64_t bd = b0 + (uint64_t)((t * C::CH + 2 * j) * N);
-                                umma::mma_bf16(d, ad, bd, idesc, g > 0 || t > 0 || j > 0);
+                                for (int j = 0; j < C::CH / 2; ++j) {
+                                    const uint64_t ad = ar + (uint64_t)(2 * j * (C::PLANE / 16) + dx);
+                                    const uint64_t bt = b0 + (uint64_t)((dx * C::CH + 2 * j) * 3 * N);
+                                    if (dx == 0 && j == 0 && fresh) {
+                                        umma::mma_bf16(acc + (uint32_t)(sr * N), ad, bt + 2 * N, id1, false);
+                                        if (lo < sr) umma::mma_bf16(dlo, ad, bt + boff, rows == 3 ? id2 : id1, true);
+                                    } else {
+                                        umma::mma_bf16(dlo, ad, bt + boff, idn, true);
+                                    }
+                                }
+                            }
+                        }
+                    } else {
+                        const uint64_t a0 = desc(st, C::PLANE, 128), b0 = desc(st + C::IN, N * 16, 128);
+#pragma unroll 1
+                        for (int r = 0; r < C::R; ++r) {
+                            const uint64_t ar = a0 + (uint64_t)(r * (kRow / 16));
+                            const uint32_t d = acc + (uint32_t)(r * N);
+#pragma unroll
+                            for (int t = 0; t < 9; ++t) {
+                                constexpr int kRow16 = kRow / 16;
+                                const int dy = t / 3, dx = t % 3;  // input row r + dy, pixel offset dx (staged from -1)
+#pragma unroll
+                                for (int j = 0; j < C::CH / 2; ++j) {
+                                    const uint64_t ad = ar + (uint64_t)(2 * j * (C::PLANE / 16) + dy * kRow16 + dx);
+                                    const uint64_t bd = b0 + (uint64_t)((t * C::CH + 2 * j) * N);
+                                    umma::mma_bf16(d, ad, bd, idesc, g > 0 || t > 0 || j > 0);
+                                }
                             }
                         }
                     }
@@ -378,14 +428,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
         }
         __syncwarp();
     } else {
-        // ------------------------------------------------------------------ epilogue (warps 2-9)
-        // the accumulator of a block is R x N columns = R N / 16 units of 16 columns (unit u: output
-        // row u / (N / 16), channels 16 (u % (N / 16)) ..); warp w reads tensor-memory lanes
-        // 32 (w % 4) .. (its 32 pixels) and takes every other pair of units, so two warps share each
-        // lane quarter; a pair is two loads and one wait
+        // ------------------------------------------------------------------ epilogue (warps 2-17)
+        // the accumulator of a block is R x N columns = R N / 32 pairs of 16-column units (unit u:
+        // output row u / (N / 16), channels 16 (u % (N / 16)) ..); warp w reads tensor-memory lanes
+        // 32 (w % 4) .. (its 32 pixels), so four warps share each lane quarter and take every fourth
+        // pair (two loads, one wait)
         constexpr int kPairs = C::R * N / 32;
+        constexpr int kMine = (kPairs + 3) / 4;  // pairs per warp, at most
         static_assert(C::R * N % 32 == 0, "whole pairs of 16-column units");
-        const int quad = warp & 3, half = (warp - 2) >> 2;
+        const int quad = warp & 3, part = (warp - 2) >> 2;
         const int px = quad * 32 + lane;
         int a = 0;
         uint32_t aphase = 0;
@@ -399,8 +450,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int x = x0 + px;
             const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)a * kAccCols;
-#pragma unroll 1
-            for (int pr = half; pr < kPairs; pr += 2) {
+#pragma unroll
+            for (int i = 0; i < kMine; ++i) {
+                const int pr = part + 4 * i;  // warp-uniform
+                if (pr >= kPairs) break;
                 float v[32];
                 umma::tmem_ld16_issue(lane_base + (uint32_t)(pr * 32), v);
                 umma::tmem_ld16_issue(lane_base + (uint32_t)(pr * 32 + 16), v + 16);
@@ -427,9 +480,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2u * kAccCols) : "memory");
 }
 
-// Weights of one layer in the order the kernel streams them: wt[g][t][c][n][e] = w[n][t * cin + g G + 8 c + e]
-// (zero past cin or cout). w: [cout][kp] bf16, K index k = tap * cin + ci.
-__global__ void k_conv3_arrange(const bf16* w, int cout, int cin, int kp, int N, int G, int groups, bf16* wt) {
+// Weights of one layer in the order the kernel streams them (zero past cin or cout; w: [cout][kp]
+// bf16, K index k = tap * cin + ci, tap = 3 dy + dx):
+//   wt[g][t][c][n][e]      = w[n][t * cin + g G + 8 c + e]                     (N >= 96)
+//   wt[g][dx][c][s][n][e]  = w[n][(3 (2 - s) + dx) * cin + g G + 8 c + e]      (stacked, N <= 64)
+__global__ void k_conv3_arrange(const bf16* w, int cout, int cin, int kp, int N, int G, int groups, int stack,
+                                bf16* wt) {
     const int CH = G / 8;
     const long total = (long)groups * 9 * CH * N * 8;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
@@ -438,10 +494,21 @@ __global__ void k_conv3_arrange(const bf16* w, int cout, int cin, int kp, int N,
         q /= 8;
         const int n = (int)(q % N);
         q /= N;
-        const int c = (int)(q % CH);
-        q /= CH;
-        const int t = (int)(q % 9);
-        const int g = (int)(q / 9);
+        int t, c, g;
+        if (stack) {
+            const int s3 = (int)(q % 3);
+            q /= 3;
+            c = (int)(q % CH);
+            q /= CH;
+            const int dx = (int)(q % 3);
+            g = (int)(q / 3);
+            t = 3 * (2 - s3) + dx;
+        } else {
+            c = (int)(q % CH);
+            q /= CH;
+            t = (int)(q % 9);
+            g = (int)(q / 9);
+        }
         const int ci = g * G + c * 8 + e;
         bf16 v = __float2bfloat16_rn(0.0f);
         if (n < cout && ci < cin) v = w[(size_t)n * kp + t * cin + ci];
@@ -458,7 +525,7 @@ static int n_of(int cout) {
     if (cout <= 128) return 128;
     return 192;
 }
-static int g_of(int N) { return N >= 192 ? 16 : 32; }
+static int g_of(int N, int cin) { return 8 * chs_of(N, cin); }
 
 static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     static std::once_flag once;
@@ -473,9 +540,9 @@ static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     return fn;
 }
 
-template <int N>
+template <int N, int CHS>
 static cudaError_t launch(const bf16* x, int ldx, int xoff, int cin, const Params& prm, cudaStream_t st) {
-    using Cf = Cfg<N>;
+    using Cf = Cfg<N, CHS>;
     auto enc = encoder();
     if (!enc) return cudaErrorNotSupported;
     // 4-D view of the chunk-planar activations as 8-byte elements: (2 W, H, chunk, B), the chunks of
@@ -504,11 +571,11 @@ static cudaError_t launch(const bf16* x, int ldx, int xoff, int cin, const Param
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaFuncSetAttribute(k_conv3<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cf::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_conv3<N, CHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cf::SMEM);
     if (e != cudaSuccess) return e;
     const int grid = q.blocks < sms ? q.blocks : sms;
     if (grid <= 0) return cudaSuccess;
-    k_conv3<N><<<grid, kThreads, Cf::SMEM, st>>>(map, tail, q);
+    k_conv3<N, CHS><<<grid, kThreads, Cf::SMEM, st>>>(map, tail, q);
     return cudaGetLastError();
 }
 
@@ -523,17 +590,18 @@ extern "C" {
 // Bytes of the arranged weights of a layer with cout outputs and cin inputs (see k_conv3_arrange).
 unsigned long long gpsb_dn_conv3_weight_bytes(int cout, int cin) {
     if (cout < 1 || cout > 192 || cin < 1) return 0;
-    const int N = n_of(cout), G = g_of(N);
+    const int N = n_of(cout), G = g_of(N, cin);
     return (unsigned long long)((cin + G - 1) / G) * 9ull * (G / 8) * N * 16ull;
 }
 
 // Arranges w ([cout][kp] bf16, k = tap * cin + ci) into wt (gpsb_dn_conv3_weight_bytes bytes).
 int gpsb_dn_conv3_weights(const void* w, int cout, int cin, int kp, void* wt, void* stream) {
     if (cout < 1 || cout > 192 || cin < 1 || kp < 9 * cin || !w || !wt) return (int)cudaErrorInvalidValue;
-    const int N = n_of(cout), G = g_of(N), groups = (cin + G - 1) / G;
+    const int N = n_of(cout), G = g_of(N, cin), groups = (cin + G - 1) / G;
     const long total = (long)groups * 9 * (G / 8) * N * 8;
     const int blocks = (int)((total + 255) / 256 < 1184 ? (total + 255) / 256 : 1184);
-    k_conv3_arrange<<<blocks, 256, 0, (cudaStream_t)stream>>>((const bf16*)w, cout, cin, kp, N, G, groups, (bf16*)wt);
+    k_conv3_arrange<<<blocks, 256, 0, (cudaStream_t)stream>>>((const bf16*)w, cout, cin, kp, N, G, groups,
+                                                              3 * N <= 256 ? 1 : 0, (bf16*)wt);
     return (int)cudaGetLastError();
 }
 
@@ -563,13 +631,14 @@ int gpsb_dn_conv3(const void* x, int ldx, int xoff, int cin, int B, int H, int W
     prm.err = err;
     const bf16* xb = (const bf16*)x;
     cudaStream_t st = (cudaStream_t)stream;
+    const bool narrow = chs_of(32, cin) == 2;  // cin <= 16: two chunk planes per stage
     switch (n_of(cout)) {
-        case 16: return (int)launch<16>(xb, ldx, xoff, cin, prm, st);
-        case 32: return (int)launch<32>(xb, ldx, xoff, cin, prm, st);
-        case 64: return (int)launch<64>(xb, ldx, xoff, cin, prm, st);
-        case 96: return (int)launch<96>(xb, ldx, xoff, cin, prm, st);
-        case 128: return (int)launch<128>(xb, ldx, xoff, cin, prm, st);
-        default: return (int)launch<192>(xb, ldx, xoff, cin, prm, st);
+        case 16: return (int)(narrow ? launch<16, 2>(xb, ldx, xoff, cin, prm, st) : launch<16, 4>(xb, ldx, xoff, cin, prm, st));
+        case 32: return (int)(narrow ? launch<32, 2>(xb, ldx, xoff, cin, prm, st) : launch<32, 4>(xb, ldx, xoff, cin, prm, st));
+        case 64: return (int)(narrow ? launch<64, 2>(xb, ldx, xoff, cin, prm, st) : launch<64, 4>(xb, ldx, xoff, cin, prm, st));
+        case 96: return (int)(narrow ? launch<96, 2>(xb, ldx, xoff, cin, prm, st) : launch<96, 4>(xb, ldx, xoff, cin, prm, st));
+        case 128: return (int)(narrow ? launch<128, 2>(xb, ldx, xoff, cin, prm, st) : launch<128, 4>(xb, ldx, xoff, cin, prm, st));
+        default: return (int)launch<192, 2>(xb, ldx, xoff, cin, prm, st);
     }
 }
 

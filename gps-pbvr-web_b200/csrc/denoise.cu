@@ -246,20 +246,19 @@ __global__ void k_relu_bwd(const float* g, int ldg, int goff, const bf16* y, int
 }
 
 // nearest 2x upsampling of src (chunk-planar, lds channels, B x h x w) channels [0, C) into dst
-// (chunk-planar, ldd channels, B x 2h x 2w) channels [doff, doff + C)
-__global__ void k_up2(const bf16* src, int lds, int B, int h, int w, int C, bf16* dst, int ldd, int doff) {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int H = 2 * h, W = 2 * w;
-    if (i >= (long)B * H * W * C) return;
-    const int e = (int)(i & 7);
-    long t = i >> 3;
-    const int X = (int)(t % W);
-    t /= W;
-    const int Y = (int)(t % H);
-    t /= H;
-    const int ch = (int)(t % (C / 8)), b = (int)(t / (C / 8));
-    dst[((((size_t)b * (ldd / 8) + doff / 8 + ch) * H + Y) * W + X) * 8 + e] =
-        src[((((size_t)b * (lds / 8) + ch) * h + Y / 2) * w + X / 2) * 8 + e];
+// (chunk-planar, ldd channels, B x 2h x 2w) channels [doff, doff + C): one thread per 16-byte
+// source pixel slot (8 channels), grid (ceil(w / 128), h, B C / 8), four 16-byte stores
+__global__ void __launch_bounds__(128) k_up2(const uint4* src, int lds, int h, int w, int C, uint4* dst, int ldd,
+                                             int doff) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w) return;
+    const int nch = C / 8, b = blockIdx.z / nch, ch = blockIdx.z - b * nch, W = 2 * w;
+    const uint4 v = src[(((size_t)b * (lds / 8) + ch) * h + y) * w + x];
+    uint4* d = dst + (((size_t)b * (ldd / 8) + doff / 8 + ch) * (2 * (size_t)h) + 2 * y) * W + 2 * x;
+    d[0] = v;
+    d[1] = v;
+    d[W] = v;
+    d[W + 1] = v;
 }
 // out (B, h, w, C) = sum over each 2x2 block of g (B, 2h, 2w, ldg) channels [goff, goff + C)
 __global__ void k_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int C, float* out) {
@@ -273,23 +272,35 @@ __global__ void k_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w
     out[i] = s;
 }
 // 2x2 average pooling of src (chunk-planar, lds channels, B x 2h x 2w) channels [soff, soff + C) into
-// dst (chunk-planar, C channels, B x h x w)
-__global__ void k_pool2(const bf16* src, int lds, int soff, int B, int h, int w, int C, bf16* dst) {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long)B * h * w * C) return;
-    const int e = (int)(i & 7);
-    long t = i >> 3;
-    const int x = (int)(t % w);
-    t /= w;
-    const int y = (int)(t % h);
-    t /= h;
-    const int ch = (int)(t % (C / 8)), b = (int)(t / (C / 8));
-    const int H = 2 * h, W = 2 * w;
-    const bf16* s0 = src + (((size_t)b * (lds / 8) + soff / 8 + ch) * H) * W * 8;
-    float s = 0.0f;
+// dst (chunk-planar, C channels, B x h x w): one thread per 16-byte destination pixel slot, grid
+// (ceil(w / 128), h, B C / 8); each channel sums its four inputs in the order (2y, 2x), (2y, 2x+1),
+// (2y+1, 2x), (2y+1, 2x+1) in fp32 and stores a quarter of the sum
+__global__ void __launch_bounds__(128) k_pool2(const uint4* src, int lds, int soff, int h, int w, int C, uint4* dst) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w) return;
+    const int nch = C / 8, b = blockIdx.z / nch, ch = blockIdx.z - b * nch, W = 2 * w;
+    const uint4* s0 = src + (((size_t)b * (lds / 8) + soff / 8 + ch) * (2 * (size_t)h) + 2 * y) * W + 2 * x;
+    const uint4 q[4] = {s0[0], s0[1], s0[W], s0[W + 1]};
+    float acc[8];
 #pragma unroll
-    for (int d = 0; d < 4; ++d) s += __bfloat162float(s0[((size_t)(2 * y + (d >> 1)) * W + 2 * x + (d & 1)) * 8 + e]);
-    dst[i] = __float2bfloat16_rn(0.25f * s);
+    for (int e = 0; e < 8; ++e) acc[e] = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        const uint32_t wd[4] = {q[d].x, q[d].y, q[d].z, q[d].w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&wd[k]));
+            acc[2 * k] += f.x;
+            acc[2 * k + 1] += f.y;
+        }
+    }
+    uint32_t o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        __nv_bfloat162 hh = __floats2bfloat162_rn(0.25f * acc[2 * k], 0.25f * acc[2 * k + 1]);
+        o[k] = *reinterpret_cast<uint32_t*>(&hh);
+    }
+    dst[(((size_t)b * nch + ch) * h + y) * w + x] = make_uint4(o[0], o[1], o[2], o[3]);
 }
 // acc (B, 2h, 2w, lda) channels [aoff, aoff + C) += g (B, h, w, C) / 4 spread over each 2x2 block
 __global__ void k_pool2_bwd_add(const float* g, int B, int h, int w, int C, float* acc, int lda, int aoff) {
@@ -509,9 +520,11 @@ int gpsb_dn_relu_bwd(const float* g, int ldg, int goff, const void* y, int ldy, 
     return (int)cudaGetLastError();
 }
 int gpsb_dn_up2(const void* src, int lds, int B, int h, int w, int C, void* dst, int ldd, int doff, void* stream) {
-    if (C % 8 || lds % 8 || ldd % 8 || doff % 8) return (int)cudaErrorInvalidValue;
-    k_up2<<<grid_of(4L * B * h * w * C), 256, 0, (cudaStream_t)stream>>>((const bf16*)src, lds, B, h, w, C, (bf16*)dst,
-                                                                          ldd, doff);
+    if (C % 8 || lds % 8 || ldd % 8 || doff % 8 || B < 1 || h < 1 || w < 1 || h > 65535 || (long)B * (C / 8) > 65535 ||
+        ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u))
+        return (int)cudaErrorInvalidValue;
+    k_up2<<<dim3((w + 127) / 128, h, B * (C / 8)), 128, 0, (cudaStream_t)stream>>>((const uint4*)src, lds, h, w, C,
+                                                                                   (uint4*)dst, ldd, doff);
     return (int)cudaGetLastError();
 }
 int gpsb_dn_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int C, float* out, void* stream) {
@@ -519,9 +532,11 @@ int gpsb_dn_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int 
     return (int)cudaGetLastError();
 }
 int gpsb_dn_pool2(const void* src, int lds, int soff, int B, int h, int w, int C, void* dst, void* stream) {
-    if (C % 8 || lds % 8 || soff % 8) return (int)cudaErrorInvalidValue;
-    k_pool2<<<grid_of((long)B * h * w * C), 256, 0, (cudaStream_t)stream>>>((const bf16*)src, lds, soff, B, h, w, C,
-                                                                             (bf16*)dst);
+    if (C % 8 || lds % 8 || soff % 8 || B < 1 || h < 1 || w < 1 || h > 65535 || (long)B * (C / 8) > 65535 ||
+        ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u))
+        return (int)cudaErrorInvalidValue;
+    k_pool2<<<dim3((w + 127) / 128, h, B * (C / 8)), 128, 0, (cudaStream_t)stream>>>((const uint4*)src, lds, soff, h, w,
+                                                                                     C, (uint4*)dst);
     return (int)cudaGetLastError();
 }
 int gpsb_dn_pool2_bwd_add(const float* g, int B, int h, int w, int C, float* acc, int lda, int aoff, void* stream) {

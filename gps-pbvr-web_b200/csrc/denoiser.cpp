@@ -61,8 +61,20 @@ struct gpsb_denoiser {
     // activations of the current frame size (batch 1)
     uint32_t W = 0, H = 0;
     Buf x, base, feat, a1, cat1, p1, a2, cat2, p2, a3, b3, d2a, d2, d1a, d1, r, pred, err, sum;
+    // the U-Net's 16 launches captured once per frame size and replayed as one graph launch (the
+    // kernels' arguments, tensor maps included, are fixed for fixed buffers)
+    cudaStream_t capture = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    uint32_t graph_w = 0, graph_h = 0;
+    bool graph_unavailable = false;  // a capture failed: keep launching directly
     std::string error;
 };
+
+static void drop_graph(gpsb_denoiser* d) {
+    if (d->graph) cudaGraphExecDestroy(d->graph);
+    d->graph = nullptr;
+    d->graph_w = d->graph_h = 0;
+}
 
 static gpsb_status dn_fail(gpsb_denoiser* d, gpsb_status s, const std::string& msg) {
     if (d) d->error = msg;
@@ -93,6 +105,8 @@ gpsb_status gpsb_denoiser_create(int device, gpsb_denoiser** out) {
 void gpsb_denoiser_destroy(gpsb_denoiser* d) {
     if (!d) return;
     cudaSetDevice(d->device);
+    drop_graph(d);
+    if (d->capture) cudaStreamDestroy(d->capture);
     for (int l = 0; l < GPSB_DN_LAYERS; ++l) {
         d->wt[l].release();
         d->bias[l].release();
@@ -117,6 +131,7 @@ gpsb_status gpsb_denoiser_set_layer(gpsb_denoiser* d, uint32_t layer, const floa
     if (!d || !w || !b || layer >= GPSB_DN_LAYERS) return dn_fail(d, GPSB_ERR_INVALID_ARGUMENT, "bad layer or null");
     const Layer& L = kLayers[layer];
     cudaSetDevice(d->device);
+    drop_graph(d);
     const int K = 9 * L.cin, kp = (K + 63) / 64 * 64;
     // fp32 rows [cout][kp] on the device, then bf16, then the conv3 arrangement
     Buf wf, wb;
@@ -149,6 +164,7 @@ gpsb_status gpsb_denoiser_set_gate(gpsb_denoiser* d, float gate_limit) {
 
 static gpsb_status ensure_frame(gpsb_denoiser* d, uint32_t W, uint32_t H) {
     if (d->W == W && d->H == H && d->x.p) return GPSB_OK;
+    drop_graph(d);
     const size_t P = (size_t)W * H, P2 = P / 4, P4 = P / 16;
     const size_t bf = 2;
     struct {
@@ -196,6 +212,42 @@ static gpsb_status unet(gpsb_denoiser* d, cudaStream_t st) {
     return GPSB_OK;
 }
 
+// The U-Net on st: the captured graph of this frame size, or (first frame of a size) the direct
+// launches followed by one capture of the same launches on the denoiser's own stream.
+static gpsb_status run_unet(gpsb_denoiser* d, cudaStream_t st) {
+    if (d->graph && d->graph_w == d->W && d->graph_h == d->H) {
+        DCK(d, cudaGraphLaunch(d->graph, st), "graph launch");
+        return GPSB_OK;
+    }
+    gpsb_status s = unet(d, st);
+    if (s != GPSB_OK || d->graph_unavailable) return s;
+    if (!d->capture && cudaStreamCreateWithFlags(&d->capture, cudaStreamNonBlocking) != cudaSuccess) {
+        d->capture = nullptr;
+        d->graph_unavailable = true;
+        cudaGetLastError();
+        return GPSB_OK;
+    }
+    cudaGraph_t g = nullptr;
+    bool ok = cudaStreamBeginCapture(d->capture, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        const std::string keep = d->error;
+        const bool launched = unet(d, d->capture) == GPSB_OK;
+        d->error = keep;
+        ok = cudaStreamEndCapture(d->capture, &g) == cudaSuccess && launched && g &&
+             cudaGraphInstantiate(&d->graph, g, 0) == cudaSuccess;
+    }
+    if (g) cudaGraphDestroy(g);
+    if (ok) {
+        d->graph_w = d->W;
+        d->graph_h = d->H;
+    } else {
+        d->graph = nullptr;
+        d->graph_unavailable = true;
+        cudaGetLastError();
+    }
+    return GPSB_OK;
+}
+
 static gpsb_status check_loaded(gpsb_denoiser* d) {
     for (int l = 0; l < GPSB_DN_LAYERS; ++l)
         if (!d->loaded[l]) return dn_fail(d, GPSB_ERR_STATE, std::string("layer ") + kLayers[l].name + " not set");
@@ -219,7 +271,7 @@ gpsb_status gpsb_denoiser_forward(gpsb_denoiser* d, const void* x_dev, const flo
     DCK(d, cudaMemcpyAsync(d->x.p, x_dev, P * 16, cudaMemcpyDeviceToDevice, st), "input");
     DCK(d, cudaMemcpyAsync(d->base.p, base_dev, P * 12, cudaMemcpyDeviceToDevice, st), "input");
     DCK(d, cudaMemsetAsync(d->err.p, 0, 4, st), "error word");
-    s = unet(d, st);
+    s = run_unet(d, st);
     if (s != GPSB_OK) return s;
     DCK(d, cudaMemcpyAsync(pred_dev, d->pred.p, P * 12, cudaMemcpyDeviceToDevice, st), "output");
     uint32_t e = 0;
@@ -269,7 +321,7 @@ gpsb_status gpsb_render_denoised(gpsb_renderer* r, gpsb_denoiser* d, const gpsb_
     if (used_denoiser) *used_denoiser = use ? 1 : 0;
     if (use) {
         DCK(d, cudaMemsetAsync(d->err.p, 0, 4, st), "error word");
-        s = unet(d, st);
+        s = run_unet(d, st);
         if (s != GPSB_OK) return s;
         DCK(d, cudaMemcpyAsync(rgb_host, d->pred.p, P * 12, cudaMemcpyDeviceToHost, st), "read frame");
         uint32_t e = 0;
