@@ -10,40 +10,46 @@
 //
 //   Y[b][y][x][n] = act(bias[n] + sum_{dy,dx,ci} X[b][y+dy][x+dx][ci] W[n][(dy+1)*3 + (dx+1)][ci])
 //
-// Work unit ("block"): R output rows x one 128-pixel row segment of one image, all N output
+// Work unit ("block"): R output rows x one 126-pixel row segment of one image, all N output
 // channels. The K loop runs over groups of G input channels. One pipeline stage holds
-//   * the R + 2 input rows y0-1 .. y0+R of pixels x0-1 .. x0+128 of the group's channels, one
-//     plane per 8-channel chunk: [chunk][row][pixel][8 channels], 16 bytes per (row, pixel), rows
-//     kRow = 2176 bytes apart (130 pixels used, padded so every row starts 128-byte aligned). TMA
-//     splits a box into one request per innermost box row, so the chunk-planar tensor is viewed
-//     as 8-byte elements (2 per pixel): each staged row is one 2048-byte box (128 pixels) and one
-//     32-byte box (the last 2 halo pixels), issued by the lanes of the producer warp; pixels and
-//     rows outside the image read as zeros (TMA out-of-bounds fill), which is the padding;
+//   * the R + 2 input rows y0-1 .. y0+R of the 128 pixels x0-1 .. x0+126 of the group's channels,
+//     one plane per 8-channel chunk: [chunk][row][pixel][8 channels], 16 bytes per (row, pixel),
+//     rows 2048 bytes apart. The chunk-planar tensor is viewed as 8-byte elements (2 per pixel) so
+//     that the whole stage, 256 elements x (R + 2) rows x CH planes, is ONE TMA box: a TMA copy
+//     costs about 80 clocks however small it is, and one copy per staged row (plus one for the
+//     halo pixels a 128-pixel segment would need) bounded the narrow layers. Pixels, rows and
+//     chunks outside the tensor read as zeros (TMA out-of-bounds fill), which is the padding;
 //   * the group's weights in the canonical K-major layout of the MMA's B operand, one 1-D bulk copy
-//     of a block that gpsb_dn_conv3_weights arranged once: [tap][chunk][n][8 channels].
+//     of a block that gpsb_dn_conv3_weights arranged once.
 // In the canonical K-major layout without swizzle a core matrix is 8 rows x 16 bytes, i.e. eight
 // consecutive pixels of one chunk plane; the MMA of output row r, tap (dy, dx) and chunk pair j
-// reads A from plane 2j, row r + dy + 1, starting at pixel dx + 1 (leading byte offset = the plane
-// size, stride byte offset = 128 bytes): the nine taps are nine descriptors over the same staged
-// rows, so each input byte crosses from L2 once per block instead of nine times.
+// reads A from plane 2j, row r + dy, starting at pixel dx (leading byte offset = the plane size,
+// stride byte offset = 128 bytes): the nine taps are nine descriptors over the same staged rows,
+// so each input byte crosses from L2 once per block instead of nine times. The MMA's M = 128 rows
+// are output pixels x0 .. x0+127; the last two read past their staged row (into the next row, or
+// for the last row of the last plane into the first bytes of the stage's weights) and are not
+// stored, which is why a segment is 126 pixels.
 //
-// A tensor-core MMA of M = 128, K = 16 costs about 50 clocks however small N is (it reads the 4 KB
-// A tile from shared memory each time), so for N <= 64 the three vertical taps share one MMA of
-// width 3 N: staged row sr feeds output rows sr - 2 .. sr, whose accumulators are consecutive
-// column blocks, through B = the taps dy = 2, 1, 0 stacked (weights arranged [dx][chunk][dy][n][8]);
-// that is (R + 2) x 3 MMAs per chunk pair instead of R x 9.
+// Cost of one MMA of M = 128, K = 16 (measured on B200, clocks): max(32 + N / 4, N / 2, ~40) on the
+// tensor core (the 4 KB A tile and the N x 32-byte B tile read from shared memory at 128 bytes per
+// clock, or the math), and about 54 clocks of issue for one thread. Narrow layers therefore
+//   * stack the three vertical taps in one MMA when 3 N <= 256: staged row sr feeds output rows
+//     sr - 2 .. sr, whose accumulators are consecutive column blocks, through B = the taps
+//     dy = 2, 1, 0 stacked (weights arranged [dx][chunk][dy][n][8]), (R + 2) x 3 MMAs per chunk
+//     pair instead of R x 9;
+//   * for N <= 32, issue from two threads, each for its own half of the accumulator rows (the
+//     stacked schedule clipped to those rows), so the order of every accumulation stays fixed.
 //
-// Roles (persistent CTAs, one per SM, 576 threads): warp 0 issues the TMA copies, one thread of
-// warp 1 issues the MMAs (M = 128 pixels, N, K = 16) into one of two tensor-memory accumulators of
-// R x N fp32 columns, warps 2-17 read the other accumulator back (tcgen05.ld, warp w reads lanes
+// Roles (persistent CTAs, one per SM, 608 threads): warp 0 issues the TMA copies, lane 0 of warps 1
+// (and 2) issues the MMAs (M = 128 pixels, N, K = 16) into one of two tensor-memory accumulators of
+// R x N fp32 columns, warps 3-18 read the other accumulator back (tcgen05.ld, warp w reads lanes
 // 32 (w % 4) .., four warps per lane quarter taking every fourth 32-column pair, two loads per
-// wait) and apply bias (staged once per CTA in shared memory), ReLU and the bf16 /
-// fp32 store, so the epilogue of block i overlaps the MMAs of block i + 1. Stages and accumulators
-// hand over through mbarriers (TMA
-// transaction counts, tcgen05.commit, epilogue arrivals). Every wait is bounded: a wait that gives
-// up sets bit CONV3_ERR_TIMEOUT in the caller's error word and raises an abort flag that ends every
-// role; the CTA then waits (bounded) for its own TMA copies and MMAs before it frees its tensor
-// memory and returns. No cluster, no multicast.
+// wait) and apply bias (staged once per CTA in shared memory), ReLU and the bf16 / fp32 store, so
+// the epilogue of block i overlaps the MMAs of block i + 1. Stages and accumulators hand over
+// through mbarriers (TMA transaction counts, tcgen05.commit of each issuer, epilogue arrivals).
+// Every wait is bounded: a wait that gives up sets bit CONV3_ERR_TIMEOUT in the caller's error word
+// and raises an abort flag that ends every role; the CTA then waits (bounded) for its own TMA copies
+// and MMAs before it frees its tensor memory and returns. No cluster, no multicast.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -59,11 +65,12 @@ namespace c3 {
 
 using bf16 = __nv_bfloat16;
 
-constexpr int kSeg = 128;             // output pixels of a row segment (the MMA's M)
-constexpr int kHalo = kSeg + 2;       // staged input pixels per row
-constexpr int kRow = 2176;            // bytes between staged rows: 130 x 16 used, 128-byte aligned
-constexpr int kThreads = 576;         // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
+constexpr int kSeg = 126;             // output pixels of a row segment (the MMA's M = 128, 2 unused)
+constexpr int kStaged = 128;          // staged input pixels per row: x0 - 1 .. x0 + 126
+constexpr int kRow = kStaged * 16;    // bytes of a staged row
+constexpr int kThreads = 608;         // warp 0 TMA, warps 1-2 MMA, warps 3-18 epilogue
 constexpr int kEpiWarps = 16;         // four per tensor-memory lane quarter
+constexpr int kEpiWarp0 = 3;          // first epilogue warp
 constexpr uint32_t kAccCols = 256;    // tensor-memory columns of one accumulator (two are allocated)
 constexpr uint32_t kSpin = 1u << 24;  // polls of a bounded wait
 constexpr uint32_t CONV3_ERR_TIMEOUT = 32u;
@@ -79,13 +86,20 @@ struct Cfg {
     static constexpr int CH = CHS;                                       // chunk planes per stage
     static constexpr int G = 8 * CH;
     static constexpr bool STACK = 3 * N <= 256;
+    // MMA-issuing threads: one thread issues at most one M = 128 MMA per ~54 clocks, while the
+    // tensor core finishes one of N <= 32 in ~40 (its 4 KB A read), so for N <= 32 two threads
+    // issue, each for its own half of the accumulator rows
+    static constexpr int ISSUERS = (STACK && R == 8) ? 2 : 1;
     static constexpr int PLANE = (R + 2) * kRow;                         // bytes of one chunk plane
     static constexpr int IN = CH * PLANE;                                // staged input rows of a stage
     static constexpr int WB = 9 * CH * N * 16;                           // weight bytes of one group
-    static constexpr int STAGE = round_up(IN + WB, 1024);
+    static constexpr int STAGE = round_up(IN + WB, 1024);                // a stage with its group's weights
+    static constexpr int STAGE_IN = round_up(IN, 1024);                  // a stage of input rows only
     static constexpr int S = N >= 192 ? 3 : 2;
-    static constexpr uint32_t TX = (uint32_t)(CH * (R + 2) * kHalo * 16 + WB);  // bytes landing per stage
+    static constexpr uint32_t TX = (uint32_t)(IN + WB);                  // bytes landing per stage
     static constexpr size_t SMEM = (size_t)S * STAGE + 1024;             // + alignment slack
+    // the layout with every group's weights resident (one copy per CTA): S input stages + weights
+    static constexpr size_t smem_resident(int groups) { return (size_t)S * STAGE_IN + (size_t)groups * WB + 1024; }
     static_assert(R * N <= (int)kAccCols, "accumulator columns");
     static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N of one MMA");
     static_assert(SMEM <= 232448, "shared memory per CTA");
@@ -154,6 +168,7 @@ struct Params {
     int ldo, ooff, out_f32, relu;
     int B, H, W, cout, groups;
     int segs, rowblocks, blocks;
+    int resident;  // every group's weights stay in shared memory after one copy per CTA
     uint32_t* err;
 };
 
@@ -213,15 +228,18 @@ __device__ __forceinline__ void store16(const Params& p, float* v, const float* 
 
 template <int N, int CHS>
 __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ CUtensorMap xmap,
-                                                     const __grid_constant__ CUtensorMap xtail, const Params p) {
+                                                     const Params p) {
     using C = Cfg<N, CHS>;
     extern __shared__ __align__(1024) uint8_t s_raw[];
-    __shared__ __align__(8) uint64_t s_full[C::S], s_empty[C::S], s_acc_full[2], s_acc_empty[2], s_drain;
+    __shared__ __align__(8) uint64_t s_full[C::S], s_empty[C::S], s_acc_full[2], s_acc_empty[2], s_drain[2], s_wbar;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
     __shared__ __align__(16) float s_bias[N];  // bias of the N accumulator columns (0 past cout)
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_raw) + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // stage s at base + s * stride; resident weights (group g at wres + g WB) after the S stages
+    const size_t stride = p.resident ? (size_t)C::STAGE_IN : (size_t)C::STAGE;
+    uint8_t* const wres = base + (size_t)C::S * C::STAGE_IN;
 
     for (int n = tid; n < N; n += kThreads) s_bias[n] = (p.bias && n < p.cout) ? p.bias[n] : 0.0f;
     if (warp == 0) {
@@ -233,13 +251,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
     if (tid == 32) {
         for (int s = 0; s < C::S; ++s) {
             bar_init(&s_full[s], 1);
-            bar_init(&s_empty[s], 1);
+            bar_init(&s_empty[s], C::ISSUERS);
         }
         for (int a = 0; a < 2; ++a) {
-            bar_init(&s_acc_full[a], 1);
+            bar_init(&s_acc_full[a], C::ISSUERS);
             bar_init(&s_acc_empty[a], kEpiWarps);
         }
-        bar_init(&s_drain, 1);
+        bar_init(&s_drain[0], 1);
+        bar_init(&s_drain[1], 1);
+        bar_init(&s_wbar, 1);
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -264,72 +284,77 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
 
     if (warp == 0) {
         // ------------------------------------------------------------------ TMA producer
-        // lane 0 waits for a free stage and arms its barrier; the 32 lanes then issue the stage's
-        // (R + 2) x CH row pairs (a 2048-byte box and a 32-byte box each); lane 0 adds the weights
-        uint32_t armed = 0;  // stages armed at least once (for the abort drain)
+        // lane 0: wait for a free stage, arm its barrier, issue the stage's one input box and the
+        // group's weights
         if (lane == 0) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
-            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xtail)) : "memory");
-        }
-        int stage = 0;
-        uint32_t phase = 0;
-        bool stop = false;
-        for (int blk = blockIdx.x; blk < p.blocks && !stop; blk += gridDim.x) {
-            int b, y0, x0;
-            decode(blk, b, y0, x0);
-            for (int g = 0; g < p.groups; ++g) {
-                int ok = 1;
-                if (lane == 0) {
-                    ok = (!s_abort && bar_wait(&s_empty[stage], phase ^ 1u, &s_abort)) ? 1 : 0;
-                    if (!ok) fail();
-                    else bar_expect(&s_full[stage], C::TX);
-                }
-                ok = __shfl_sync(0xffffffffu, ok, 0);
-                if (!ok) {
-                    stop = true;
-                    break;
-                }
-                uint8_t* st = base + (size_t)stage * C::STAGE;
-                for (int t = lane; t < C::CH * (C::R + 2); t += 32) {
-                    const int c = t / (C::R + 2), rr = t - c * (C::R + 2);
-                    const uint32_t row = saddr(st + c * C::PLANE + rr * kRow);
-                    const int y = y0 - 1 + rr, ch = g * C::CH + c;
-                    tma_load4(row, &xmap, 2 * (x0 - 1), y, ch, b, &s_full[stage]);
-                    tma_load4(row + 2048u, &xtail, 2 * (x0 + kSeg - 1), y, ch, b, &s_full[stage]);
-                }
-                if (lane == 0) bulk_load(saddr(st + C::IN), p.wt + (size_t)g * (C::WB / 2), (uint32_t)C::WB, &s_full[stage]);
-                armed |= 1u << stage;
-                if (++stage == C::S) {
-                    stage = 0;
-                    phase ^= 1u;
+            if (p.resident) {
+                bar_expect(&s_wbar, (uint32_t)(p.groups * C::WB));
+                for (int g = 0; g < p.groups; ++g)
+                    bulk_load(saddr(wres) + (uint32_t)(g * C::WB), p.wt + (size_t)g * (C::WB / 2), (uint32_t)C::WB, &s_wbar);
+            }
+            uint32_t armed = 0;  // stages armed at least once (for the abort drain)
+            int stage = 0;
+            uint32_t phase = 0;
+            bool stop = false;
+            for (int blk = blockIdx.x; blk < p.blocks && !stop; blk += gridDim.x) {
+                int b, y0, x0;
+                decode(blk, b, y0, x0);
+                for (int g = 0; g < p.groups; ++g) {
+                    if (s_abort || !bar_wait(&s_empty[stage], phase ^ 1u, &s_abort)) {
+                        fail();
+                        stop = true;
+                        break;
+                    }
+                    bar_expect(&s_full[stage], p.resident ? (uint32_t)C::IN : C::TX);
+                    const uint32_t st = saddr(base + (size_t)stage * stride);
+                    tma_load4(st, &xmap, 2 * (x0 - 1), y0 - 1, g * C::CH, b, &s_full[stage]);
+                    if (!p.resident)
+                        bulk_load(st + C::IN, p.wt + (size_t)g * (C::WB / 2), (uint32_t)C::WB, &s_full[stage]);
+                    armed |= 1u << stage;
+                    if (++stage == C::S) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
                 }
             }
-        }
-        __syncwarp();
-        if (lane == 0 && s_abort) {
-            // let this CTA's copies land before the CTA can exit: every stage's last armed phase
-            // completes by its transaction count alone
-            int st2 = stage;
-            uint32_t ph2 = phase;
-            for (int k = 0; k < C::S; ++k) {
-                if (--st2 < 0) {
-                    st2 = C::S - 1;
-                    ph2 ^= 1u;
+            if (s_abort) {
+                // let this CTA's copies land before the CTA can exit: every stage's last armed phase
+                // (and the resident weights' barrier) completes by its transaction count alone
+                if (p.resident) {
+                    for (uint32_t i = 0; i < kSpin && !bar_test(&s_wbar, 0); ++i) {
+                    }
                 }
-                if (armed & (1u << st2)) {
-                    for (uint32_t i = 0; i < kSpin && !bar_test(&s_full[st2], ph2); ++i) {
+                int st2 = stage;
+                uint32_t ph2 = phase;
+                for (int k = 0; k < C::S; ++k) {
+                    if (--st2 < 0) {
+                        st2 = C::S - 1;
+                        ph2 ^= 1u;
+                    }
+                    if (armed & (1u << st2)) {
+                        for (uint32_t i = 0; i < kSpin && !bar_test(&s_full[st2], ph2); ++i) {
+                        }
                     }
                 }
             }
         }
         __syncwarp();
-    } else if (warp == 1) {
-        // ------------------------------------------------------------------ MMA issuer
-        if (lane == 0) {
+    } else if (warp < kEpiWarp0) {
+        // ------------------------------------------------------------------ MMA issuers
+        // lane 0 of warp 1 + h issues the MMAs of accumulator rows [rlo, rhi] of every block
+        const int h = warp - 1;
+        constexpr int kRows = C::R / C::ISSUERS;
+        const int rlo = h * kRows, rhi = rlo + kRows - 1;
+        if (lane == 0 && h < C::ISSUERS) {
             constexpr uint32_t idesc = umma::idesc_bf16(N);
             int stage = 0, a = 0;
             uint32_t phase = 0, aphase = 0;
             bool issued = false;
+            if (p.resident) {
+                if (bar_wait(&s_wbar, 0, &s_abort)) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                else fail();
+            }
             for (int blk = blockIdx.x; blk < p.blocks && !s_abort; blk += gridDim.x) {
                 if (!bar_wait(&s_acc_empty[a], aphase ^ 1u, &s_abort)) {
                     fail();
@@ -344,7 +369,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t st = saddr(base + (size_t)stage * C::STAGE);
+                    const uint32_t st = saddr(base + (size_t)stage * stride);
+                    const uint32_t wg = p.resident ? saddr(wres) + (uint32_t)(g * C::WB) : st + C::IN;
                     // one descriptor per operand and stage; every MMA adds a compile-time byte
                     // offset / 16 to its 14-bit start-address field (shared addresses stay below
                     // 256 KB, so the field never carries into the offsets above it)
@@ -356,12 +382,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
                         // lie in consecutive N-column blocks. Output row sr is first written by staged
                         // row sr (tap dy = 0) at dx = 0, first chunk pair, group 0: that block is split
                         // off and written without accumulation.
-                        const uint64_t a0 = desc(st, C::PLANE, 128), b0 = desc(st + C::IN, 3 * N * 16, 128);
+                        const uint64_t a0 = desc(st, C::PLANE, 128), b0 = desc(wg, 3 * N * 16, 128);
                         constexpr uint32_t id1 = umma::idesc_bf16(N), id2 = umma::idesc_bf16(2 * N),
                                            id3 = umma::idesc_bf16(3 * N);
 #pragma unroll 1
-                        for (int sr = 0; sr < C::R + 2; ++sr) {
-                            const int lo = sr > 2 ? sr - 2 : 0, hi = sr < C::R - 1 ? sr : C::R - 1;
+                        for (int sr = rlo; sr < rhi + 3; ++sr) {
+                            const int lo = sr - 2 > rlo ? sr - 2 : rlo, hi = sr < rhi ? sr : rhi;
                             const int rows = hi - lo + 1;
                             const uint32_t idn = rows == 3 ? id3 : rows == 2 ? id2 : id1;
                             const uint32_t dlo = acc + (uint32_t)(lo * N);
@@ -384,9 +410,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
                             }
                         }
                     } else {
-                        const uint64_t a0 = desc(st, C::PLANE, 128), b0 = desc(st + C::IN, N * 16, 128);
+                        const uint64_t a0 = desc(st, C::PLANE, 128), b0 = desc(wg, N * 16, 128);
 #pragma unroll 1
-                        for (int r = 0; r < C::R; ++r) {
+                        for (int r = rlo; r <= rhi; ++r) {
                             const uint64_t ar = a0 + (uint64_t)(r * (kRow / 16));
                             const uint32_t d = acc + (uint32_t)(r * N);
 #pragma unroll
@@ -421,14 +447,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
             }
             // every MMA this CTA issued has completed before its tensor memory can be freed
             if (issued) {
-                umma::mma_commit(&s_drain);
-                for (uint32_t i = 0; i < kSpin && !bar_test(&s_drain, 0); ++i) {
+                umma::mma_commit(&s_drain[h]);
+                for (uint32_t i = 0; i < kSpin && !bar_test(&s_drain[h], 0); ++i) {
                 }
             }
         }
         __syncwarp();
     } else {
-        // ------------------------------------------------------------------ epilogue (warps 2-17)
+        // ------------------------------------------------------------------ epilogue (warps 3-18)
         // the accumulator of a block is R x N columns = R N / 32 pairs of 16-column units (unit u:
         // output row u / (N / 16), channels 16 (u % (N / 16)) ..); warp w reads tensor-memory lanes
         // 32 (w % 4) .. (its 32 pixels), so four warps share each lane quarter and take every fourth
@@ -436,7 +462,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
         constexpr int kPairs = C::R * N / 32;
         constexpr int kMine = (kPairs + 3) / 4;  // pairs per warp, at most
         static_assert(C::R * N % 32 == 0, "whole pairs of 16-column units");
-        const int quad = warp & 3, part = (warp - 2) >> 2;
+        const int quad = warp & 3, part = (warp - kEpiWarp0) >> 2;
         const int px = quad * 32 + lane;
         int a = 0;
         uint32_t aphase = 0;
@@ -461,7 +487,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const int u = 2 * pr + h, y = y0 + u / (N / 16), c = (u % (N / 16)) * 16;
-                    if (x < p.W && y < p.H) store16(p, v + 16 * h, s_bias + c, b, y, x, c);
+                    if (px < kSeg && x < p.W && y < p.H) store16(p, v + 16 * h, s_bias + c, b, y, x, c);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -546,36 +572,43 @@ static cudaError_t launch(const bf16* x, int ldx, int xoff, int cin, const Param
     auto enc = encoder();
     if (!enc) return cudaErrorNotSupported;
     // 4-D view of the chunk-planar activations as 8-byte elements: (2 W, H, chunk, B), the chunks of
-    // channels [xoff, xoff + cin) of a tensor of ldx channels; boxes of one staged row: 256
-    // elements (128 pixels) and 4 elements (2 pixels)
-    CUtensorMap map, tail;
+    // channels [xoff, xoff + cin) of a tensor of ldx channels; the box of one stage: 256 elements
+    // (128 pixels) x (R + 2) rows x CH chunk planes
+    CUtensorMap map;
     const cuuint64_t plane = (cuuint64_t)prm.W * prm.H * 16;  // bytes of one chunk plane
     const cuuint64_t dims[4] = {(cuuint64_t)prm.W * 2, (cuuint64_t)prm.H, (cuuint64_t)((cin + 7) / 8), (cuuint64_t)prm.B};
     const cuuint64_t strides[3] = {(cuuint64_t)prm.W * 16, plane, plane * (cuuint64_t)(ldx / 8)};
-    const cuuint32_t box[4] = {2 * kSeg, 1, 1, 1}, box_tail[4] = {4, 1, 1, 1};
+    const cuuint32_t box[4] = {2 * kStaged, (cuuint32_t)Cf::R + 2, (cuuint32_t)Cf::CH, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     void* gaddr = (void*)(x + (size_t)(xoff / 8) * prm.W * prm.H * 8);
-    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, gaddr, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r == CUDA_SUCCESS)
-        r = enc(&tail, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, gaddr, dims, strides, box_tail, estr,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, gaddr, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     Params q = prm;
     q.segs = (prm.W + kSeg - 1) / kSeg;
     q.rowblocks = (prm.H + Cf::R - 1) / Cf::R;
     q.blocks = q.segs * q.rowblocks * prm.B;
     q.groups = (cin + Cf::G - 1) / Cf::G;
-    int dev = 0, sms = 148;
+    int dev = 0, sms = 148, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaFuncSetAttribute(k_conv3<N, CHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cf::SMEM);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_conv3<N, CHS>);
     if (e != cudaSuccess) return e;
+    // the largest dynamic size this instance may use (set once to the maximum, so every launch of
+    // it, captured in a graph or not, stays within the attribute)
+    const size_t dyn_max = (size_t)optin - fa.sharedSizeBytes;
+    if (Cf::SMEM > dyn_max) return cudaErrorInvalidConfiguration;
+    e = cudaFuncSetAttribute(k_conv3<N, CHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_max);
+    if (e != cudaSuccess) return e;
+    const size_t smem_res = Cf::smem_resident(q.groups);
+    q.resident = smem_res <= dyn_max ? 1 : 0;
+    const size_t smem = q.resident ? smem_res : Cf::SMEM;
     const int grid = q.blocks < sms ? q.blocks : sms;
     if (grid <= 0) return cudaSuccess;
-    k_conv3<N, CHS><<<grid, kThreads, Cf::SMEM, st>>>(map, tail, q);
+    k_conv3<N, CHS><<<grid, kThreads, smem, st>>>(map, q);
     return cudaGetLastError();
 }
 

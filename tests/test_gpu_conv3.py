@@ -1,7 +1,7 @@
 """The TMA-staged 3x3 convolution (gpsb_dn_conv3, csrc/conv3x3.cu) on chunk-planar activations
 against PyTorch's fp32 convolution of the same bf16-rounded operands, for every output width the
 kernel instantiates (16 .. 192 channels), the input widths of the U-Net and of its data gradients
-(8 .. 192), images whose width is not a multiple of the 128-pixel segment and whose height is not a
+(8 .. 192), images whose width is not a multiple of the 126-pixel segment and whose height is not a
 multiple of the row block, batches, channel slices of wider tensors (input offset, output offset),
 bf16 (chunk-planar) and fp32 (pixel-major) outputs, bias and ReLU. Tolerance: fp32 accumulation
 order (2e-3 of the output's scale), or one bf16 rounding for bf16 outputs. The whole U-Net on
@@ -36,6 +36,9 @@ CASES = [
     (1, 9, 300, 40, 8, 24, 96, 96, 0, True, False),      # data gradient of c5a (96 out), offset input
     (1, 4, 129, 64, 0, 64, 192, 200, 8, True, False),    # data gradient of c4a (192 out), offset output
     (3, 8, 128, 8, 0, 8, 16, 16, 0, True, False),        # N = 16 with 16 outputs
+    (1, 9, 126, 32, 0, 32, 32, 32, 0, False, True),      # exactly one 126-pixel segment
+    (2, 6, 127, 64, 0, 64, 64, 64, 0, False, True),      # a second segment of one pixel
+    (1, 10, 252, 32, 0, 32, 128, 128, 0, False, False),  # two whole segments, N = 128 (taps unstacked)
 ]
 
 
