@@ -58,6 +58,7 @@
 
 #include <mutex>
 
+#include "pdl.cuh"
 #include "umma.cuh"
 
 namespace gpsb {
@@ -241,12 +242,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
     const size_t stride = p.resident ? (size_t)C::STAGE_IN : (size_t)C::STAGE;
     uint8_t* const wres = base + (size_t)C::S * C::STAGE_IN;
 
-    for (int n = tid; n < N; n += kThreads) s_bias[n] = (p.bias && n < p.cout) ? p.bias[n] : 0.0f;
+    // Launched with programmatic stream serialisation, this prologue (tensor memory, barriers, the
+    // tensor-map prefetch) overlaps the end of the previous kernel; nothing in global memory is read
+    // before the grid-dependency wait (the previous kernel may have written the input, the weights
+    // or the bias), and every write comes after it.
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&s_tmem)),
                      "r"(2u * kAccCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        if (lane == 0) asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
     }
     if (tid == 32) {
         for (int s = 0; s < C::S; ++s) {
@@ -263,6 +268,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    grid_dependency_wait();
+    launch_dependents();
+    for (int n = tid; n < N; n += kThreads) s_bias[n] = (p.bias && n < p.cout) ? p.bias[n] : 0.0f;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -287,7 +295,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv3(const __grid_constant__ C
         // lane 0: wait for a free stage, arm its barrier, issue the stage's one input box and the
         // group's weights
         if (lane == 0) {
-            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
             if (p.resident) {
                 bar_expect(&s_wbar, (uint32_t)(p.groups * C::WB));
                 for (int g = 0; g < p.groups; ++g)
@@ -608,8 +615,7 @@ static cudaError_t launch(const bf16* x, int ldx, int xoff, int cin, const Param
     const size_t smem = q.resident ? smem_res : Cf::SMEM;
     const int grid = q.blocks < sms ? q.blocks : sms;
     if (grid <= 0) return cudaSuccess;
-    k_conv3<N, CHS><<<grid, kThreads, smem, st>>>(map, q);
-    return cudaGetLastError();
+    return launch_pdl(k_conv3<N, CHS>, dim3(grid), dim3(kThreads), smem, st, map, q);
 }
 
 }  // namespace c3

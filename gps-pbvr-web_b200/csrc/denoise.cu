@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "pdl.cuh"
 #include "umma.cuh"
 
 namespace gpsb {
@@ -250,6 +251,8 @@ __global__ void k_relu_bwd(const float* g, int ldg, int goff, const bf16* y, int
 // source pixel slot (8 channels), grid (ceil(w / 128), h, B C / 8), four 16-byte stores
 __global__ void __launch_bounds__(128) k_up2(const uint4* src, int lds, int h, int w, int C, uint4* dst, int ldd,
                                              int doff) {
+    grid_dependency_wait();  // launched with programmatic stream serialisation
+    launch_dependents();
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= w) return;
     const int nch = C / 8, b = blockIdx.z / nch, ch = blockIdx.z - b * nch, W = 2 * w;
@@ -276,6 +279,8 @@ __global__ void k_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w
 // (ceil(w / 128), h, B C / 8); each channel sums its four inputs in the order (2y, 2x), (2y, 2x+1),
 // (2y+1, 2x), (2y+1, 2x+1) in fp32 and stores a quarter of the sum
 __global__ void __launch_bounds__(128) k_pool2(const uint4* src, int lds, int soff, int h, int w, int C, uint4* dst) {
+    grid_dependency_wait();  // launched with programmatic stream serialisation
+    launch_dependents();
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= w) return;
     const int nch = C / 8, b = blockIdx.z / nch, ch = blockIdx.z - b * nch, W = 2 * w;
@@ -347,6 +352,8 @@ __global__ void k_l1(const float* base, const float* r, const float* target, int
 }
 // out = base + r (M x 3)
 __global__ void k_residual(const float* base, const float* r, int n, float* out) {
+    grid_dependency_wait();  // launched with programmatic stream serialisation
+    launch_dependents();
     const int i = gtid();
     if (i < n) out[i] = base[i] + r[i];
 }
@@ -523,9 +530,8 @@ int gpsb_dn_up2(const void* src, int lds, int B, int h, int w, int C, void* dst,
     if (C % 8 || lds % 8 || ldd % 8 || doff % 8 || B < 1 || h < 1 || w < 1 || h > 65535 || (long)B * (C / 8) > 65535 ||
         ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u))
         return (int)cudaErrorInvalidValue;
-    k_up2<<<dim3((w + 127) / 128, h, B * (C / 8)), 128, 0, (cudaStream_t)stream>>>((const uint4*)src, lds, h, w, C,
-                                                                                   (uint4*)dst, ldd, doff);
-    return (int)cudaGetLastError();
+    return (int)launch_pdl(k_up2, dim3((w + 127) / 128, h, B * (C / 8)), dim3(128), 0, (cudaStream_t)stream,
+                           (const uint4*)src, lds, h, w, C, (uint4*)dst, ldd, doff);
 }
 int gpsb_dn_up2_bwd(const float* g, int ldg, int goff, int B, int h, int w, int C, float* out, void* stream) {
     k_up2_bwd<<<grid_of((long)B * h * w * C), 256, 0, (cudaStream_t)stream>>>(g, ldg, goff, B, h, w, C, out);
@@ -535,9 +541,8 @@ int gpsb_dn_pool2(const void* src, int lds, int soff, int B, int h, int w, int C
     if (C % 8 || lds % 8 || soff % 8 || B < 1 || h < 1 || w < 1 || h > 65535 || (long)B * (C / 8) > 65535 ||
         ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u))
         return (int)cudaErrorInvalidValue;
-    k_pool2<<<dim3((w + 127) / 128, h, B * (C / 8)), 128, 0, (cudaStream_t)stream>>>((const uint4*)src, lds, soff, h, w,
-                                                                                     C, (uint4*)dst);
-    return (int)cudaGetLastError();
+    return (int)launch_pdl(k_pool2, dim3((w + 127) / 128, h, B * (C / 8)), dim3(128), 0, (cudaStream_t)stream,
+                           (const uint4*)src, lds, soff, h, w, C, (uint4*)dst);
 }
 int gpsb_dn_pool2_bwd_add(const float* g, int B, int h, int w, int C, float* acc, int lda, int aoff, void* stream) {
     k_pool2_bwd_add<<<grid_of(4L * B * h * w * C), 256, 0, (cudaStream_t)stream>>>(g, B, h, w, C, acc, lda, aoff);
@@ -554,7 +559,9 @@ int gpsb_dn_l1(const float* base, const float* r, const float* target, int M, fl
     return (int)cudaGetLastError();
 }
 int gpsb_dn_residual(const float* base, const float* r, int n, float* out, void* stream) {
-    k_residual<<<grid_of(n), 256, 0, (cudaStream_t)stream>>>(base, r, n, out);
+    if (n <= 0) return (int)cudaSuccess;
+    const cudaError_t e = launch_pdl(k_residual, dim3(grid_of(n)), dim3(256), 0, (cudaStream_t)stream, base, r, n, out);
+    if (e != cudaSuccess) return (int)e;
     return (int)cudaGetLastError();
 }
 int gpsb_dn_adam(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps, int t,
