@@ -58,3 +58,12 @@ def test_reference_cameras_equal_the_renderers():
     _, cams = bench.reference_inputs()
     for (name, c17), (name2, cam) in zip(cams, bench.cameras(pkg)):
         assert name == name2 and np.array_equal(c17, cam.to_array())
+
+
+def test_equal_psnr_target_statement():
+    met = bench.equal_psnr_target(4.2, 0.45, 33.4, 396.0)
+    assert met == {"target": 8.0, "met": True, "why_not": None}
+    far = bench.equal_psnr_target(0.283, 0.45, 31.4, 30.9)
+    assert far["met"] is False and "31 ensembles" in far["why_not"] and "5.5x" in far["why_not"]
+    unknown = bench.equal_psnr_target(4.2, 0.45, 37.0, None)
+    assert unknown["met"] is None and "largest" in unknown["why_not"]
