@@ -428,6 +428,7 @@ def denoise_measure(pkg, r, stream, cams, p, per_view_ms, ref_ens=256, w=None, h
                 torch.cuda.synchronize()
                 ts.append(a.elapsed_time(b))
             dn_ms = statistics.median(ts)
+            out["graph_state"] = nat.graph_state()  # 1: the timed calls replayed the captured graph
             pred = pred.reshape(P, 3).clone()
             ps_dn, me_dn = T.psnr(pred, ref)
             view_counts = list(counts)

@@ -169,6 +169,7 @@ SIGNATURES = {
     "gpsb_denoiser_set_layer": (ST, [P, U32, P, P]),
     "gpsb_denoiser_set_gate": (ST, [P, C.c_float]),
     "gpsb_denoiser_forward": (ST, [P, P, P, U32, U32, P, P]),
+    "gpsb_denoiser_graph_state": (C.c_int, [P]),
     "gpsb_render_denoised": (ST, [P, P, P, P, U32, U32, C.c_float, U32, P, P, P]),
     "gpsb_dn_conv3_weights": (ST, [P, ST, ST, ST, P, P]),
     "gpsb_dn_conv3": (ST, [P, ST, ST, ST, ST, ST, ST, P, ST, P, P, ST, ST, ST, ST, P, P]),

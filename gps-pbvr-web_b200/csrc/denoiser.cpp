@@ -119,6 +119,12 @@ void gpsb_denoiser_destroy(gpsb_denoiser* d) {
 
 const char* gpsb_denoiser_last_error(const gpsb_denoiser* d) { return d ? d->error.c_str() : ""; }
 
+int gpsb_denoiser_graph_state(const gpsb_denoiser* d) {
+    if (!d) return 0;
+    if (d->graph_unavailable) return -1;
+    return (d->graph && d->graph_w == d->W && d->graph_h == d->H) ? 1 : 0;
+}
+
 gpsb_status gpsb_denoiser_layer_shape(uint32_t layer, uint32_t* cin, uint32_t* cin_real, uint32_t* cout) {
     if (layer >= GPSB_DN_LAYERS) return GPSB_ERR_INVALID_ARGUMENT;
     if (cin) *cin = (uint32_t)kLayers[layer].cin;

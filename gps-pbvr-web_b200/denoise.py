@@ -421,6 +421,11 @@ class NativeDenoiser:
         H, W = x.shape[1], x.shape[2]
         self._check(self._L.gpsb_denoiser_forward(self._h, _p(x), _p(base), W, H, _p(pred), _stream()))
 
+    def graph_state(self):
+        """1: the layers of the current frame size replay a captured CUDA graph; 0: not captured yet;
+        -1: a capture failed and the layers launch directly (gpsb_denoiser_graph_state)."""
+        return int(self._L.gpsb_denoiser_graph_state(self._h))
+
     def render(self, renderer, cam, params, first_seed, ensembles=4, gate_limit=0.0, fallback_ensembles=64):
         """gpsb_render_denoised: returns (rgb (H*W, 3) float32 numpy array, used_denoiser, check)."""
         import numpy as np

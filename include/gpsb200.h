@@ -504,6 +504,11 @@ gpsb_status gpsb_denoiser_set_gate(gpsb_denoiser* d, float gate_limit);
  * (x 3 fp32 mean colour) -> pred_dev (x 3 fp32). Width and height multiples of 4. Synchronous. */
 gpsb_status gpsb_denoiser_forward(gpsb_denoiser* d, const void* x_dev, const float* base_dev, uint32_t width,
                                   uint32_t height, float* pred_dev, void* cuda_stream);
+/* How the network's layers run (gpsb_denoiser_forward, gpsb_render_denoised): 1 = captured in a
+ * CUDA graph for the current frame size, later frames of that size replay it; 0 = no frame of the
+ * current size yet (the next one launches the layers and captures them); -1 = a capture failed,
+ * frames launch the layers directly. */
+int gpsb_denoiser_graph_state(const gpsb_denoiser* d);
 /* A denoised frame of renderer r (render_ensembles, crates/gps-render/src/gps.rs:861, followed by
  * the network): resets r's accumulation, renders `ensembles` ensembles (seeds first_seed..) with
  * per-pixel feature sums, packs the 8 input features and computes the variance check. When the
