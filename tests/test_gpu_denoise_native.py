@@ -52,8 +52,8 @@ def test_native_forward_equals_python_sequencing():
 
 def test_native_forward_graph_replay():
     """The first forward of a frame size launches the layers directly and captures them; later
-    forwards replay the capture. Every call, on new inputs and across a change of frame size and
-    back, equals the Python sequencing bit for bit."""
+    forwards replay the capture (gpsb_denoiser_graph_state). Every call, on new inputs and across a
+    change of frame size and back, equals the Python sequencing bit for bit."""
     dn = _dn()
     net = dn.Denoiser()
     dn.load_weights(net)
@@ -67,6 +67,7 @@ def test_native_forward_graph_replay():
         nat.forward(x, base, b)
         torch.cuda.synchronize()
         assert torch.equal(a, b), (H_, W_, (a - b).abs().max().item())
+        assert nat.graph_state() == 1  # this size's layers are captured (and replayed from now on)
     nat.close()
 
 
